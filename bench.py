@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 swept heat on one B200 (and N replicas under torchrun).
+
+Workload (one "step" = one full solve): the 2-D heat equation u_t = u_xx + u_yy
+on the periodic unit square, 8192 x 8192 FP64 cells, forward Euler with
+dt = 0.2*dx^2, 5000 time steps, swept decomposition with blocksize 32
+(15 levels per half-cycle).  The initial field is a seeded sum of 8 periodic
+Fourier modes (amplitudes U(0,1)).  The 537 MB field is larger than the
+126 MB L2, so consecutive steps do not run from cache.
+
+Reported on one JSON line (rank 0):
+  value      Gcell-updates/s of the swept path with the field resident in HBM
+  standard   the same workload through the standard (one step per launch) path
+  e2e        the same metric through the public API with host buffers: pinned
+             host -> device upload, the run, device -> host download
+  roofline   the dominant kernel's effective bandwidth (16 B per cell update:
+             read and write of one FP64 value) against the measured HBM copy
+             bandwidth; above 1.0 means temporal reuse
+  cpu_baseline  the reference's CPU swept algorithm (C restatement) on the
+             host cores, on a bounded sample of the same workload
+
+`--impl reference` times that CPU algorithm alone as the reference arm.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s FP64 swept vs standard (1 B200)"
+UNIT = "Gcell-updates/s"
+CELL_BYTES = 16  # one FP64 read + one FP64 write per cell update
+
+
+def fourier_field(n, seed=0, modes=8):
+    """Sum of `modes` periodic Fourier modes with U(0,1) amplitudes (seeded)."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(0, 1, modes)
+    k = rng.integers(1, 9, modes)
+    l = rng.integers(1, 9, modes)
+    ph = rng.uniform(0, 2 * np.pi, modes)
+    x = np.arange(n) / n
+    f = np.zeros((n, n))
+    for m in range(modes):
+        # sin(2 pi (k x + l y) + phi) = sin(A)cos(B) + cos(A)sin(B)
+        A = 2 * np.pi * k[m] * x[:, None] + ph[m]
+        B = 2 * np.pi * l[m] * x[None, :]
+        f += a[m] * (np.sin(A) * np.cos(B) + np.cos(A) * np.sin(B))
+    return f[None]
+
+
+def heat_globals(n, steps):
+    dx = 1.0 / n
+    dt = 0.2 * dx * dx
+    return [0.0, steps * dt, dt, dx, dx, 1.0, True]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows)}
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+            out["sm_max_mhz"] = max(mx) if mx else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        seen = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for nm, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        seen.add(nm)
+        out["reasons"] = sorted(seen)
+        pw = [float(r[3]) for r in self.rows if len(r) >= 9 and r[3].replace(".", "").isdigit()]
+        if pw:
+            out["power_w_max"] = max(pw)
+        return out
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kind, n, bs):
+    """DRAM bytes per launch of one kernel kind, from a committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"heat2d_swept_{kind}_traffic.txt")
+    try:
+        for line in open(p):
+            k, _, v = line.partition("=")
+            if k.strip() == f"bytes_per_launch_n{n}_bs{bs}":
+                return float(v)
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(n_sample, bs, levels_cycles, threads):
+    """The reference's CPU swept algorithm (C restatement) on a sample grid."""
+    import oracle
+    ic = fourier_field(n_sample)
+    g = heat_globals(n_sample, 10)
+    mpss = bs // 2 - 1
+    t0 = time.perf_counter()
+    oracle.swept("heat", ic, g, 1, 1, bs, max_gss=levels_cycles - 1, nthreads=threads,
+                  frames=False)
+    dt = time.perf_counter() - t0
+    cells = float(n_sample) ** 2 * mpss * levels_cycles
+    return cells / dt / 1e9, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, _ = cpu_baseline(args.ref_n, args.bs, args.ref_cycles, threads)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    sample = (f"{args.ref_n}x{args.ref_n} heat, bs {args.bs}, {args.ref_cycles} swept "
+              f"half-cycles ({(args.bs // 2 - 1) * args.ref_cycles} levels) per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args):
+    return {"workload": f"heat2d-fp64-periodic-{args.n}x{args.n}-{args.nsteps}steps-swept",
+            "n": args.n, "time_steps": args.nsteps, "blocksize": args.bs,
+            "levels_per_half_cycle": args.h or args.bs // 2 - 1, "nseg": args.nseg,
+            "l2": "inputs larger than L2 (field of n*n*8 bytes)"}
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from pysweep_b200 import Engine, plugin_constants
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, steps, bs = args.n, args.nsteps, args.bs
+    ic = fourier_field(n, seed=0)
+    g = heat_globals(n, steps)
+    eng = Engine("heat", n, n, its=1, blocksize=bs, device=local)
+    for k, v in plugin_constants("heat", g).items():
+        eng.set_global(k, v)
+    eng.configure(h=args.h, nseg=args.nseg)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    d_ic = torch.from_numpy(ic).cuda()
+    cells_per_step = float(n) * n * steps
+
+    def timed(mode, k):
+        barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = eng.launches
+        eng.profile(True)
+        ev0.record(stream)
+        for _ in range(k):
+            eng.set_state(d_ic)
+            eng.run(steps, mode=mode)
+        ev1.record(stream)
+        eng.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        ms = ev0.elapsed_time(ev1) / k
+        return max_over_ranks(ms), eng.launches - l0, eng.profile_read()
+
+    # warm-up
+    for _ in range(args.warmup):
+        eng.set_state(d_ic)
+        eng.run(steps, mode="swept")
+    eng.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_sw, launches, prof = timed("swept", args.steps)
+    clk = clocks.stop()
+    value = cells_per_step * world / (ms_sw / 1000) / 1e9
+
+    std = None
+    if args.standard_steps > 0:
+        eng.set_state(d_ic)
+        eng.run(steps, mode="standard")  # warm-up of the standard kernel
+        ms_st, _, prof_st = timed("standard", args.standard_steps)
+        std = {"value": cells_per_step * world / (ms_st / 1000) / 1e9, "ms_per_step": ms_st,
+               "steps": args.standard_steps}
+        pk = prof_st["standard"]
+        if pk[1]:
+            std["kernel_effective_gbs"] = pk[2] * CELL_BYTES / (pk[0] / 1000) / 1e9
+
+    # end to end through the public API with pinned host buffers
+    h_in = torch.from_numpy(ic).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    h_in_np, h_out_np = h_in.numpy(), h_out.numpy()
+    for _ in range(1):
+        eng.set_state(h_in_np)
+        eng.run(steps)
+        eng.get_state(out=h_out_np)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.e2e_steps):
+        eng.set_state(h_in_np)
+        eng.run(steps)
+        eng.get_state(out=h_out_np)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(ev0.elapsed_time(ev1) / args.e2e_steps)
+    e2e = {"value": cells_per_step * world / (ms_e2e / 1000) / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8),
+           "ms_per_step": ms_e2e, "steps": args.e2e_steps}
+
+    # roofline of the dominant kernel
+    kinds = {k: v for k, v in prof.items() if v[1] > 0}
+    dom = max(kinds, key=lambda k: kinds[k][0])
+    dms, dn, dcells = kinds[dom]
+    achieved = dcells * CELL_BYTES / (dms / 1000) / 1e9
+    peak, peak_src = measured_peak()
+    traffic = ncu_traffic(dom, n, bs)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "kernel": dom,
+            "launches": dn, "avg_launch_ms": dms / dn,
+            "algorithmic_bytes_per_launch": dcells * CELL_BYTES / dn,
+            "peak_source": peak_src,
+            "kernel_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()}}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_sw,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(args), "standard": std,
+            "swept_vs_standard": (value / std["value"]) if std else None,
+            "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, secs = cpu_baseline(args.ref_n, bs, args.ref_cycles, threads)
+        line["cpu_baseline"] = {
+            "value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{args.ref_n}x{args.ref_n} heat, bs {bs}, {args.ref_cycles} swept "
+                      f"half-cycles, {secs:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--nsteps", type=int, default=5000)
+    ap.add_argument("--bs", type=int, default=32)
+    ap.add_argument("--h", type=int, default=0)
+    ap.add_argument("--nseg", type=int, default=1)
+    ap.add_argument("--standard-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-n", type=int, default=2048)
+    ap.add_argument("--ref-cycles", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

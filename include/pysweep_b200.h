@@ -1,0 +1,159 @@
+/*
+ * pysweep_b200 -- C ABI of the B200 swept space-time solver.
+ *
+ * One ps_solver owns the device state of one periodic 2-D field
+ * ([nv][nx][ny] doubles, C order, the reference's (v, x, y) layout without
+ * the time axis), the buffers the swept and standard decompositions need, and
+ * one CUDA stream.  Calls on one solver are serialised by the caller; solvers
+ * on different host threads are independent.  Every entry point returns
+ * PS_OK (0) or a negative PS_ERR_* code; nothing aborts the process and no
+ * call blocks on the device unless its description says so.  Host pointers
+ * are borrowed for the duration of the call only.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the anthony-walker/pysweep checkout).
+ */
+#ifndef PYSWEEP_B200_H
+#define PYSWEEP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PS_OK 0
+#define PS_ERR_INVALID (-1)     /* bad argument or configuration */
+#define PS_ERR_CUDA (-2)        /* a CUDA runtime/driver call failed */
+#define PS_ERR_NOMEM (-3)       /* device allocation failed */
+#define PS_ERR_TIMEOUT (-4)     /* a bounded device-side wait gave up */
+#define PS_ERR_UNSUPPORTED (-5) /* configuration this build does not provide */
+#define PS_ERR_COMPILE (-6)     /* a user step hook failed to compile */
+#define PS_ERR_STATE (-7)       /* call out of order (e.g. run before set_state) */
+
+/* built-in equations (the reference's plugins, pysweep/equations/*.py + *.cu) */
+#define PS_EQ_HEAT 0
+#define PS_EQ_EULER 1
+#define PS_EQ_EXAMPLE 2
+#define PS_EQ_CHECKER 3
+#define PS_EQ_HALF 4
+
+/* decompositions (yaml key "swept", pysweep/core/io.py:46) */
+#define PS_MODE_SWEPT 0
+#define PS_MODE_STANDARD 1
+
+typedef struct ps_solver ps_solver;
+
+/*
+ * Create a solver for an nv x nx x ny periodic field.
+ * Replaces the device half of block.sweptBlock/standardBlock
+ * (pysweep/core/block.py:21-43, 64-104, 193-213): context creation,
+ * GPU array allocation and the framework constants of io.copyConstants
+ * (pysweep/core/io.py:169-184).  ops = stencil half-width ("operating_points"),
+ * its = intermediate stages ("intermediate_steps"), blocksize = bs
+ * (MPSS = bs/(2*ops) - 1, pysweep/core/solver.py:119).
+ */
+int ps_create(ps_solver **out, int device, int equation, int nv, int nx, int ny, int ops, int its,
+              int blocksize);
+
+/* Release everything the solver owns.  Replaces process.cleanupProcesses'
+ * context pop (pysweep/core/process.py:28-33). */
+int ps_destroy(ps_solver *s);
+
+/*
+ * Set a named plugin constant (e.g. "DT", "DX", "DY", "ALPHA", "SCHEME",
+ * "GAMMA", "GAM_M1", "DTDX", "DTDY").  Replaces
+ * source_mod.get_global(name) + cuda.memcpy_htod(ptr, value) in the plugins'
+ * set_globals (pysweep/equations/heat.py:38-46, euler.py:25-31).  nbytes is
+ * 8 for a double, 4 for an int32, 1 for a bool; the value is converted to the
+ * constant's type.
+ */
+int ps_set_global(ps_solver *s, const char *name, const void *value, size_t nbytes);
+
+/*
+ * Look up a named constant: *size receives its size in bytes and *handle an
+ * opaque handle usable with ps_set_global_handle.  Framework constants
+ * (NV, SX, SY, VARS, TIMES, MPSS, MOSS, OPS, ITS; pysweep/core/pysweep.cu:12-20)
+ * are readable through ps_get_global_value.  Replaces
+ * SourceModule.get_global (pysweep/equations/heat.py:43).
+ */
+int ps_get_global(ps_solver *s, const char *name, void **handle, size_t *size);
+int ps_set_global_handle(ps_solver *s, void *handle, const void *value, size_t nbytes);
+int ps_get_global_value(ps_solver *s, const char *name, double *value);
+
+/*
+ * Tiling knobs of the swept decomposition (0 keeps the current value):
+ * h = levels per half-cycle (1..MPSS), nseg = column blocks per row band,
+ * chunk = streaming chunk width (32 or 64), threads = threads per CTA.
+ * The defaults reproduce the reference's MPSS with bs-row bands.
+ */
+int ps_configure(ps_solver *s, int h, int nseg, int chunk, int threads);
+
+/*
+ * Upload the initial condition.  src holds `levels` fields of nv*nx*ny
+ * doubles, oldest first; with levels == 1 the field is copied to every base
+ * level, as sweptBlock/standardBlock fill sharedArray[i] for i < ITS
+ * (pysweep/core/block.py:24-25, 218-221).  src_on_device != 0 means src is a
+ * device pointer.  Replaces the memcpy_htod of the GPU window
+ * (pysweep/core/functions.py:21-22).
+ */
+int ps_set_state(ps_solver *s, const double *src, int levels, int src_on_device);
+
+/*
+ * Advance nlevels levels (nlevels = steps * its).  The level computed first is
+ * seen by the step function as globalTimeStep = gts0 (the reference starts at
+ * 1, pysweep/core/solver.py:162).  If frames != NULL, every frame_every-th
+ * completed full step k (k % its == 0 levels) is stored at
+ * frames[k/frame_every - 1] ([frame_cap][nv][nx][ny]), the levels
+ * io.sweptWrite/standardWrite select (pysweep/core/io.py:134-144, 186-208);
+ * frames_on_device != 0 means frames is a device pointer (else the copies go
+ * through the solver's stream and the call returns after they land).
+ * Replaces solver.sweptSolve / standardSolve (pysweep/core/solver.py:158-189)
+ * with the phase sequence FirstPrism/UpPrism/LastPrism
+ * (pysweep/core/functions.py:12-88) and Geometry.callGPU
+ * (pysweep/core/geometry.py:38-46).  Asynchronous with respect to the host
+ * when frames is NULL or on the device.
+ */
+int ps_run(ps_solver *s, int mode, int64_t nlevels, int gts0, double *frames, int64_t frame_cap,
+           int frame_every, int frames_on_device);
+
+/* Copy base level `level` (0 = newest, 1 = the one before) to dst.
+ * Replaces the memcpy_dtoh after each phase group (functions.py:32). */
+int ps_get_state(ps_solver *s, double *dst, int level, int dst_on_device);
+
+/* Wait for all work queued on the solver's stream; returns the first device
+ * error seen (PS_ERR_TIMEOUT when a bounded wait gave up). */
+int ps_synchronize(ps_solver *s);
+
+/* Use the given cudaStream_t (NULL = the solver's own stream). */
+int ps_set_stream(ps_solver *s, void *stream);
+
+/*
+ * Per-kernel device timing.  ps_profile(s, 1) resets the counters and brackets
+ * every following launch with CUDA events on the solver's stream;
+ * ps_profile_read returns, for one kernel kind (0 prism stream, 1 Y-bridge
+ * seam, 2 gap stream, 3 octahedron seam, 4 standard step), the summed device
+ * time in ms, the number of launches and the algorithmic cell updates those
+ * launches performed.  Both synchronise the stream.  No reference
+ * counterpart: the reference times whole runs only (pysweep/core/io.py:10-27).
+ */
+int ps_profile(ps_solver *s, int enable);
+int ps_profile_read(ps_solver *s, int kind, double *ms, int64_t *launches, double *cells);
+
+/* Kernels launched by this solver so far (all entry points together). */
+int64_t ps_kernel_launches(const ps_solver *s);
+
+/* Last error message of this solver (never NULL); with s == NULL, the message
+ * of the last failed ps_create on this thread. */
+const char *ps_last_error(const ps_solver *s);
+
+/* Library version string. */
+const char *ps_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYSWEEP_B200_H */

@@ -1,0 +1,249 @@
+// Built-in per-cell update functions ("step hooks") for the swept and
+// standard engines.
+//
+// Each functor has the shape of the reference's GPU hook
+//   __device__ void step(double* state, int idx, int globalTimeStep)
+// (pysweep/core/pysweep.cu:25, pysweep/equations/heat.cu:35-48): it reads the
+// current level around one cell and the level before it (for the Runge-Kutta
+// roll-back), and writes the next level of that cell.  Because the swept engine
+// keeps only a ring of levels in shared memory, the three levels are passed as
+// three pointers instead of one pointer plus a TIMES stride; neighbours are at
+// fixed element offsets (Nbr), like idx +- SY and idx +- 1 in the reference.
+//
+// Arithmetic follows the numpy CPU plugins operation by operation so that the
+// GPU result is bitwise the CPU oracle's:
+//   Heat     pysweep/equations/heat.py:21-31, :48-64
+//   Euler    pysweep/equations/euler.py:131-313 (x**2 evaluated as x*x)
+//   Example  pysweep/equations/example.py:13-26
+//   Checker  pysweep/equations/checker.py:13-33
+//   Half     pysweep/equations/half.py:15-19, :35-39
+// The library is compiled with --fmad=false; fma() appears only where it is
+// exactly equal to the separately rounded expression (a - 2*c: 2*c is exact).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace psb {
+
+struct EqParams {
+    double d[8];
+    int i[4];
+};
+
+// Element offsets of the points at distance k-2 along x (rows) and y (columns).
+struct Nbr {
+    int x[5];
+    int y[5];
+    int vs;  // variable stride
+};
+
+enum EqId { EQ_HEAT = 0, EQ_EULER = 1, EQ_EXAMPLE = 2, EQ_CHECKER = 3, EQ_HALF = 4 };
+
+// heat.py: d[0] = courant = alpha*dt/dx/dx, i[0] = scheme (1 forward Euler, 0 RK2)
+struct Heat {
+    static constexpr int OPS = 1;
+    static constexpr int ID = EQ_HEAT;
+    __device__ static __forceinline__ void step(const double* __restrict__ u,
+                                                const double* __restrict__ up,
+                                                double* __restrict__ o, const Nbr& n, int gts,
+                                                int nv, const EqParams& p)
+    {
+        const double c = u[0];
+        const double cr = p.d[0];
+        const double dxx = __dmul_rn(cr, __dadd_rn(__fma_rn(-2.0, c, u[n.x[3]]), u[n.x[1]]));
+        const double dyy = __dmul_rn(cr, __dadd_rn(__fma_rn(-2.0, c, u[n.y[3]]), u[n.y[1]]));
+        const double cd = __dadd_rn(dxx, dyy);
+        if (p.i[0]) {
+            o[0] = __dadd_rn(cd, c);
+        } else {
+            const bool full = (gts % 2 == 0);
+            o[0] = __dadd_rn(__dmul_rn(full ? 1.0 : 0.5, cd), full ? up[0] : c);
+        }
+    }
+};
+
+// half.py: (u[x+1]-2u+u[x-1])/100 + (u[y+1]-2u+u[y-1])/100, RK2 on gts%2
+struct Half {
+    static constexpr int OPS = 1;
+    static constexpr int ID = EQ_HALF;
+    __device__ static __forceinline__ void step(const double* __restrict__ u,
+                                                const double* __restrict__ up,
+                                                double* __restrict__ o, const Nbr& n, int gts,
+                                                int nv, const EqParams& p)
+    {
+        const double c = u[0];
+        const double a = __ddiv_rn(__dadd_rn(__fma_rn(-2.0, c, u[n.x[3]]), u[n.x[1]]), 100.0);
+        const double b = __ddiv_rn(__dadd_rn(__fma_rn(-2.0, c, u[n.y[3]]), u[n.y[1]]), 100.0);
+        const bool full = (gts % 2 == 0);
+        o[0] = __dadd_rn(full ? up[0] : c, __dmul_rn(full ? 1.0 : 0.5, __dadd_rn(a, b)));
+    }
+};
+
+// example.py: i[0] = scheme; forward: u+1; RK2: u[t-tc] + (2 or 1)
+template <int OPS_>
+struct ExampleT {
+    static constexpr int OPS = OPS_;
+    static constexpr int ID = EQ_EXAMPLE;
+    __device__ static __forceinline__ void step(const double* __restrict__ u,
+                                                const double* __restrict__ up,
+                                                double* __restrict__ o, const Nbr& n, int gts,
+                                                int nv, const EqParams& p)
+    {
+        for (int v = 0; v < nv; ++v) {
+            const int q = v * n.vs;
+            if (p.i[0]) {
+                o[q] = __dadd_rn(u[q], 1.0);
+            } else {
+                const bool full = (gts % 2 == 0);
+                o[q] = __dadd_rn(full ? up[q] : u[q], full ? 2.0 : 1.0);
+            }
+        }
+    }
+};
+
+// checker.py: (((u[x+1] + u[x-1]) + u[y+1]) + u[y-1]) / 4
+template <int OPS_>
+struct CheckerT {
+    static constexpr int OPS = OPS_;
+    static constexpr int ID = EQ_CHECKER;
+    __device__ static __forceinline__ void step(const double* __restrict__ u,
+                                                const double* __restrict__ up,
+                                                double* __restrict__ o, const Nbr& n, int gts,
+                                                int nv, const EqParams& p)
+    {
+        for (int v = 0; v < nv; ++v) {
+            const int q = v * n.vs;
+            double s = __dadd_rn(u[q + n.x[3]], u[q + n.x[1]]);
+            s = __dadd_rn(s, u[q + n.y[3]]);
+            s = __dadd_rn(s, u[q + n.y[1]]);
+            o[q] = __ddiv_rn(s, 4.0);
+        }
+    }
+};
+
+// ------------------------------------------------------------------ Euler --
+// euler.py: d[0] = dtdx, d[1] = dtdy, d[2] = gamma, d[3] = gamma - 1
+namespace euler {
+
+__device__ __forceinline__ double pressure(double gm1, double q0, double q1, double q2, double q3)
+{
+    // euler.py:293  gM1*(q[3]-(q[1]*q[1]+q[2]*q[2])/(2*q[0]))
+    return __dmul_rn(gm1, __dsub_rn(q3, __ddiv_rn(__dadd_rn(__dmul_rn(q1, q1), __dmul_rn(q2, q2)),
+                                                  __dmul_rn(2.0, q0))));
+}
+
+// euler.py:250-256
+__device__ __forceinline__ void limiter(const double* s1, const double* s2, double num, double den,
+                                        double* out)
+{
+    double pr = __ddiv_rn(num, den);
+    if (isnan(pr) || isinf(pr) || pr > 1e6 || pr < 0.0) pr = 0.0;
+    const double h = __dmul_rn(1.0 < pr ? 1.0 : pr, 0.5);  // min(Pr,1)/2, exact halving
+#pragma unroll
+    for (int v = 0; v < 4; ++v) out[v] = __dadd_rn(s1[v], __dmul_rn(h, __dsub_rn(s2[v], s1[v])));
+}
+
+// evaluateFluxInX / evaluateFluxInY (euler.py:181-241); DIR 1 = x, 2 = y
+template <int DIR>
+__device__ __forceinline__ void flux(double gm1, const double* L, const double* R, double* f)
+{
+    const double pl = pressure(gm1, L[0], L[1], L[2], L[3]);
+    const double pr = pressure(gm1, R[0], R[1], R[2], R[3]);
+    constexpr int A = DIR;          // normal momentum component
+    constexpr int B = 3 - DIR;      // tangential momentum component
+    f[0] = __dadd_rn(L[A], R[A]);
+    const double nn = __dadd_rn(__dadd_rn(__dadd_rn(__ddiv_rn(__dmul_rn(L[A], L[A]), L[0]), pl),
+                                          __ddiv_rn(__dmul_rn(R[A], R[A]), R[0])),
+                                pr);
+    const double nt = __dadd_rn(__ddiv_rn(__dmul_rn(L[1], L[2]), L[0]),
+                                __ddiv_rn(__dmul_rn(R[1], R[2]), R[0]));
+    f[A] = nn;
+    f[B] = nt;
+    f[3] = __dadd_rn(__ddiv_rn(__dmul_rn(__dadd_rn(L[3], pl), L[A]), L[0]),
+                     __ddiv_rn(__dmul_rn(__dadd_rn(R[3], pr), R[A]), R[0]));
+}
+
+// evaluateSpectral (euler.py:258-282)
+template <int DIR>
+__device__ __forceinline__ void spectral(double gamma, double gm1, const double* L,
+                                         const double* R, double* s)
+{
+    const double rl = __dsqrt_rn(L[0]), rr = __dsqrt_rn(R[0]);
+    const double denom = __ddiv_rn(1.0, __dadd_rn(rl, rr));
+    double sp[4];
+    sp[0] = __dmul_rn(rl, rr);
+#pragma unroll
+    for (int v = 1; v < 4; ++v) {
+        const double tl = __ddiv_rn(L[v], L[0]);
+        const double tr = __ddiv_rn(R[v], R[0]);
+        sp[v] = __dmul_rn(__dadd_rn(__dmul_rn(rl, tl), __dmul_rn(rr, tr)), denom);
+    }
+    const double p = pressure(gm1, sp[0], __dmul_rn(sp[0], sp[1]), __dmul_rn(sp[0], sp[2]),
+                              __dmul_rn(sp[0], sp[3]));
+    double rad = __dadd_rn(__dsqrt_rn(__ddiv_rn(__dmul_rn(gamma, p), sp[0])), fabs(sp[DIR]));
+    if (isnan(rad)) rad = 0.0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) s[v] = __dmul_rn(rad, __dsub_rn(L[v], R[v]));
+}
+
+// getFluxInX / getFluxInY for one cell (euler.py:158-223): o[k] = offset of
+// the point at distance k-2 along the direction.
+template <int DIR>
+__device__ __forceinline__ void dflux(double gamma, double gm1, const double* __restrict__ u,
+                                      const int* o, int vs, double* out)
+{
+    double q[5][4], P[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) q[k][v] = u[o[k] + v * vs];
+        P[k] = pressure(gm1, q[k][0], q[k][1], q[k][2], q[k][3]);
+    }
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    double L[4], R[4], f[4], s[4];
+    limiter(q[1], q[2], __dsub_rn(P[2], P[1]), __dsub_rn(P[1], P[0]), L);
+    limiter(q[2], q[1], __dsub_rn(P[2], P[1]), __dsub_rn(P[3], P[2]), R);
+    flux<DIR>(gm1, L, R, f);
+    spectral<DIR>(gamma, gm1, L, R, s);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[v] = __dadd_rn(__dadd_rn(acc[v], f[v]), s[v]);
+    limiter(q[2], q[3], __dsub_rn(P[3], P[2]), __dsub_rn(P[2], P[1]), L);
+    limiter(q[3], q[2], __dsub_rn(P[3], P[2]), __dsub_rn(P[4], P[3]), R);
+    flux<DIR>(gm1, L, R, f);
+    spectral<DIR>(gamma, gm1, L, R, s);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        acc[v] = __dsub_rn(__dsub_rn(acc[v], f[v]), s[v]);
+        out[v] = __dmul_rn(acc[v], 0.5);
+    }
+}
+
+}  // namespace euler
+
+struct Euler {
+    static constexpr int OPS = 2;
+    static constexpr int ID = EQ_EULER;
+    __device__ static __forceinline__ void step(const double* __restrict__ u,
+                                                const double* __restrict__ up,
+                                                double* __restrict__ o, const Nbr& n, int gts,
+                                                int nv, const EqParams& p)
+    {
+        double fx[4], fy[4];
+        euler::dflux<1>(p.d[2], p.d[3], u, n.x, n.vs, fx);
+        euler::dflux<2>(p.d[2], p.d[3], u, n.y, n.vs, fy);
+        const double dtdx = p.d[0], dtdy = p.d[1];
+        if (gts % 2 == 0) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                o[v * n.vs] = __dadd_rn(up[v * n.vs],
+                                        __dadd_rn(__dmul_rn(fx[v], dtdx), __dmul_rn(fy[v], dtdy)));
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                o[v * n.vs] = __dadd_rn(
+                    u[v * n.vs],
+                    __dmul_rn(0.5, __dadd_rn(__dmul_rn(fx[v], dtdx), __dmul_rn(fy[v], dtdy))));
+        }
+    }
+};
+
+}  // namespace psb

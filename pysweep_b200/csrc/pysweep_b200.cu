@@ -1,0 +1,777 @@
+// C ABI of the B200 swept space-time solver (declarations: include/pysweep_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/pysweep_b200.h"
+#include "equations.cuh"
+#include "swept.cuh"
+
+namespace psb {
+
+// ---------------------------------------------------------- standard ------
+// One level of the standard decomposition (pysweep/core/pysweep.cu:259-275,
+// functions.py:126-146): every cell of level L+1 from levels L and L-1, with
+// periodic neighbours taken directly instead of through padded halos.
+template <class Eq>
+__global__ void __launch_bounds__(256) standard_kernel(const double* __restrict__ cur,
+                                                       const double* __restrict__ prev,
+                                                       double* __restrict__ out,
+                                                       double* __restrict__ frame, int nx, int ny,
+                                                       int nv, int gts, EqParams p)
+{
+    const int y = blockIdx.x * blockDim.x + threadIdx.x;
+    const int x = blockIdx.y;
+    if (y >= ny) return;
+    Nbr n;
+    n.vs = nx * ny;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        int xx = x + k - 2, yy = y + k - 2;
+        xx += xx < 0 ? nx : (xx >= nx ? -nx : 0);
+        yy += yy < 0 ? ny : (yy >= ny ? -ny : 0);
+        n.x[k] = (xx - x) * ny;
+        n.y[k] = yy - y;
+    }
+    const size_t c = (size_t)x * ny + y;
+    Eq::step(cur + c, prev + c, out + c, n, gts, nv, p);
+    if (frame) {
+        for (int v = 0; v < nv; ++v) frame[c + (size_t)v * n.vs] = out[c + (size_t)v * n.vs];
+    }
+}
+
+}  // namespace psb
+
+using namespace psb;
+
+struct ps_solver {
+    int device = 0;
+    int eq = 0;
+    int nv = 1, nx = 0, ny = 0, ops = 1, its = 1, bs = 0;
+    int mpss = 0;
+    // tiling
+    int H = 0, nseg = 1, chunk = 32, threads = 256;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // named plugin constants
+    std::map<std::string, double> globals;
+    // device buffers
+    double* base[2] = {nullptr, nullptr};  // [its][nv][nx][ny] each
+    int cur = 0;                           // which base holds the current levels
+    bool have_state = false;
+    double* xface = nullptr;
+    size_t xface_n = 0;
+    double* yface = nullptr;
+    size_t yface_n = 0;
+    double* ring[3] = {nullptr, nullptr, nullptr};
+    int64_t launches = 0;
+    std::string err;
+    // optional per-kernel device timing (ps_profile): events around every launch
+    bool profile = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double prof_ms[8] = {0};
+    int64_t prof_n[8] = {0};
+    // algorithmic cell updates per kernel kind, accumulated with prof_ms
+    double prof_cells[8] = {0};
+};
+
+namespace {
+
+const char* kVersion = "pysweep_b200 0.1.0 (sm_100a)";
+thread_local std::string g_create_error;  // message of the last failed ps_create
+
+// Opt a kernel into the large dynamic shared-memory carve-out, once per device.
+template <class K>
+void allow_big_smem(K kernel)
+{
+    static unsigned done = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(done >> dev & 1u)) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        done |= 1u << dev;
+    }
+}
+
+int fail(ps_solver* s, int code, const char* fmt, ...)
+{
+    if (s) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        s->err = buf;
+    }
+    return code;
+}
+
+#define PS_CUDA(s, call)                                                                       \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail((s), e_ == cudaErrorMemoryAllocation ? PS_ERR_NOMEM : PS_ERR_CUDA,     \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+size_t field_elems(const ps_solver* s) { return (size_t)s->nv * s->nx * s->ny; }
+
+int eq_ops(int eq, int ops)
+{
+    switch (eq) {
+    case PS_EQ_HEAT: return 1;
+    case PS_EQ_HALF: return 1;
+    case PS_EQ_EULER: return 2;
+    default: return ops;  // example / checker take the configured ops
+    }
+}
+
+// Equation constants, computed on the host the way each plugin's set_globals
+// computes its CPU globals (heat.py:37, euler.py:23-24).
+EqParams make_params(const ps_solver* s)
+{
+    EqParams p;
+    memset(&p, 0, sizeof p);
+    auto g = [&](const char* k, double d) {
+        auto it = s->globals.find(k);
+        return it == s->globals.end() ? d : it->second;
+    };
+    switch (s->eq) {
+    case PS_EQ_HEAT: {
+        const double alpha = g("ALPHA", 1.0), dt = g("DT", 0.0), dx = g("DX", 1.0);
+        p.d[0] = alpha * dt / dx / dx;
+        p.i[0] = g("SCHEME", 1.0) != 0.0;
+        break;
+    }
+    case PS_EQ_EULER: {
+        const double dt = g("DT", 0.0), dx = g("DX", 1.0), dy = g("DY", dx);
+        const double gamma = g("GAMMA", 1.4);
+        p.d[0] = g("DTDX", dt / dx);
+        p.d[1] = g("DTDY", dt / dy);
+        p.d[2] = gamma;
+        p.d[3] = g("GAM_M1", gamma - 1.0);
+        break;
+    }
+    case PS_EQ_EXAMPLE:
+    case PS_EQ_CHECKER: p.i[0] = g("SCHEME", 1.0) != 0.0; break;
+    default: break;
+    }
+    return p;
+}
+
+// ------------------------------------------------------------ dispatch ----
+using SweptLaunch = void (*)(const SweptArgs&, int grid, size_t smem, cudaStream_t);
+using StdLaunch = void (*)(const double*, const double*, double*, double*, int, int, int, int,
+                           const EqParams&, cudaStream_t);
+
+template <class Eq, int ITS, int W, bool GAP>
+void launch_stream(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
+{
+    auto k = stream_kernel<Eq, ITS, W, GAP, 256>;
+    allow_big_smem(k);
+    k<<<grid, 256, smem, st>>>(a);
+}
+
+template <class Eq, int ITS, bool GAP>
+void launch_seam(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
+{
+    auto k = seam_kernel<Eq, ITS, GAP, 128>;
+    allow_big_smem(k);
+    k<<<grid, 128, smem, st>>>(a);
+}
+
+template <class Eq>
+void launch_standard(const double* cur, const double* prev, double* out, double* frame, int nx,
+                     int ny, int nv, int gts, const EqParams& p, cudaStream_t st)
+{
+    dim3 grid((ny + 255) / 256, nx);
+    standard_kernel<Eq><<<grid, 256, 0, st>>>(cur, prev, out, frame, nx, ny, nv, gts, p);
+}
+
+struct SweptSet {
+    SweptLaunch P, Y, G, O;
+};
+
+template <class Eq, int ITS, int W>
+SweptSet make_set()
+{
+    return SweptSet{launch_stream<Eq, ITS, W, false>, launch_seam<Eq, ITS, false>,
+                    launch_stream<Eq, ITS, W, true>, launch_seam<Eq, ITS, true>};
+}
+
+// (equation, ops, its, chunk) -> kernels; nullptr members = not built.
+bool pick_swept(int eq, int ops, int its, int chunk, SweptSet* out)
+{
+#define PS_SET(EQ, OP, IT, W, T) \
+    if (eq == EQ && ops == OP && its == IT && chunk == W) { *out = make_set<T, IT, W>(); return true; }
+    PS_SET(PS_EQ_HEAT, 1, 1, 32, Heat)
+    PS_SET(PS_EQ_HEAT, 1, 2, 32, Heat)
+    PS_SET(PS_EQ_HEAT, 1, 1, 64, Heat)
+    PS_SET(PS_EQ_HEAT, 1, 2, 64, Heat)
+    PS_SET(PS_EQ_EULER, 2, 2, 32, Euler)
+    PS_SET(PS_EQ_HALF, 1, 1, 32, Half)
+    PS_SET(PS_EQ_HALF, 1, 2, 32, Half)
+    PS_SET(PS_EQ_EXAMPLE, 1, 1, 32, ExampleT<1>)
+    PS_SET(PS_EQ_EXAMPLE, 1, 2, 32, ExampleT<1>)
+    PS_SET(PS_EQ_EXAMPLE, 2, 1, 32, ExampleT<2>)
+    PS_SET(PS_EQ_EXAMPLE, 2, 2, 32, ExampleT<2>)
+    PS_SET(PS_EQ_CHECKER, 1, 1, 32, CheckerT<1>)
+    PS_SET(PS_EQ_CHECKER, 1, 2, 32, CheckerT<1>)
+    PS_SET(PS_EQ_CHECKER, 2, 1, 32, CheckerT<2>)
+    PS_SET(PS_EQ_CHECKER, 2, 2, 32, CheckerT<2>)
+#undef PS_SET
+    return false;
+}
+
+StdLaunch pick_standard(int eq, int ops)
+{
+    switch (eq) {
+    case PS_EQ_HEAT: return launch_standard<Heat>;
+    case PS_EQ_EULER: return launch_standard<Euler>;
+    case PS_EQ_HALF: return launch_standard<Half>;
+    case PS_EQ_EXAMPLE: return ops == 2 ? launch_standard<ExampleT<2>> : launch_standard<ExampleT<1>>;
+    case PS_EQ_CHECKER: return ops == 2 ? launch_standard<CheckerT<2>> : launch_standard<CheckerT<1>>;
+    default: return nullptr;
+    }
+}
+
+int check_launch(ps_solver* s)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(s, PS_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+    s->launches++;
+    return PS_OK;
+}
+
+cudaEvent_t take_event(ps_solver* s)
+{
+    if (!s->event_pool.empty()) {
+        cudaEvent_t e = s->event_pool.back();
+        s->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Kernel kinds for ps_profile_read: 0 prism stream, 1 Y-bridge seam, 2 gap
+// stream, 3 octahedron seam, 4 standard step.
+template <class F>
+int timed_launch(ps_solver* s, int kind, double cells, F&& launch)
+{
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (s->profile) {
+        a = take_event(s);
+        b = take_event(s);
+        cudaEventRecord(a, s->stream);
+    }
+    launch();
+    int rc = check_launch(s);
+    if (s->profile) {
+        cudaEventRecord(b, s->stream);
+        s->pending.push_back({kind, {a, b}});
+        s->prof_cells[kind] += cells;
+    }
+    return rc;
+}
+
+int drain_profile(ps_solver* s)
+{
+    for (auto& p : s->pending) {
+        float ms = 0.f;
+        cudaError_t e = cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+        if (e != cudaSuccess) return fail(s, PS_ERR_CUDA, "event timing: %s", cudaGetErrorString(e));
+        s->prof_ms[p.first] += ms;
+        s->prof_n[p.first] += 1;
+        s->event_pool.push_back(p.second.first);
+        s->event_pool.push_back(p.second.second);
+    }
+    s->pending.clear();
+    return PS_OK;
+}
+
+int ensure_swept_buffers(ps_solver* s)
+{
+    const int O2 = 2 * s->ops;
+    const int nb = s->nx / s->bs;
+    const int HF = std::max(s->H - 1, 0);
+    const size_t xn = (size_t)nb * HF * 2 * s->nv * O2 * s->ny;
+    const size_t yn = (size_t)nb * s->nseg * 2 * HF * s->nv * s->bs * O2;
+    if (xn > s->xface_n) {
+        if (s->xface) cudaFree(s->xface);
+        s->xface = nullptr;
+        s->xface_n = 0;
+        if (xn) PS_CUDA(s, cudaMalloc(&s->xface, xn * sizeof(double)));
+        s->xface_n = xn;
+    }
+    if (yn > s->yface_n) {
+        if (s->yface) cudaFree(s->yface);
+        s->yface = nullptr;
+        s->yface_n = 0;
+        if (yn) PS_CUDA(s, cudaMalloc(&s->yface, yn * sizeof(double)));
+        s->yface_n = yn;
+    }
+    return PS_OK;
+}
+
+size_t stream_smem(const ps_solver* s)
+{
+    const int O2 = 2 * s->ops, RS = s->chunk + O2;
+    return sizeof(double) * ((size_t)(s->its + 1) * s->nv * s->bs * RS +
+                             (size_t)(s->H + 1) * s->nv * s->bs * O2);
+}
+
+size_t seam_smem(const ps_solver* s)
+{
+    const int TW = 2 * s->ops * (s->H + 1);
+    return sizeof(double) * (size_t)(s->its + 1) * s->nv * s->bs * TW;
+}
+
+int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t frame_cap,
+              int frame_every)
+{
+    SweptSet K;
+    if (!pick_swept(s->eq, s->ops, s->its, s->chunk, &K))
+        return fail(s, PS_ERR_UNSUPPORTED, "no swept kernels for equation %d ops %d its %d chunk %d",
+                    s->eq, s->ops, s->its, s->chunk);
+    const int O2 = 2 * s->ops;
+    if (s->H < 1 || s->H > s->mpss) return fail(s, PS_ERR_INVALID, "levels per half-cycle %d not in [1, %d]", s->H, s->mpss);
+    if (s->chunk < O2 * (s->H + 1))
+        return fail(s, PS_ERR_INVALID, "chunk %d narrower than 2*ops*(h+1) = %d", s->chunk, O2 * (s->H + 1));
+    if (s->ny % s->nseg || (s->ny / s->nseg) % s->chunk)
+        return fail(s, PS_ERR_INVALID, "ny %d not divisible into %d segments of whole %d-column chunks",
+                    s->ny, s->nseg, s->chunk);
+    const size_t smem = std::max(stream_smem(s), seam_smem(s));
+    if (smem > 227 * 1024)
+        return fail(s, PS_ERR_UNSUPPORTED, "tile needs %zu bytes of shared memory", smem);
+    int rc = ensure_swept_buffers(s);
+    if (rc) return rc;
+    SweptArgs a;
+    memset(&a, 0, sizeof a);
+    a.frames = frames;
+    a.frame_cap = frames ? frame_cap : 0;
+    a.frame_every = frame_every > 0 ? frame_every : 1;
+    a.nx = s->nx;
+    a.ny = s->ny;
+    a.nv = s->nv;
+    a.bx = s->bs;
+    a.hx = s->bs / 2;
+    a.Hmax = s->H;
+    a.nb = s->nx / s->bs;
+    a.nseg = s->nseg;
+    a.wy = s->ny / s->nseg;
+    a.nchunks = a.wy / s->chunk;
+    a.its = s->its;
+    a.gts_base = gts0 - 1;
+    a.xface = s->xface;
+    a.yface = s->yface;
+    a.p = make_params(s);
+    const int units = a.nb * a.nseg;
+    const size_t fe = field_elems(s);
+    int off = 0;
+    int64_t done = 0;
+    while (done < nlevels) {
+        const int H = (int)std::min<int64_t>(s->H, nlevels - done);
+        a.H = H;
+        a.L0 = done;
+        a.off = off;
+        a.bin = s->base[s->cur];
+        a.bout = s->base[1 - s->cur];
+        if (H < s->its) {
+            // the newest its-H base levels carry over unchanged
+            for (int q = 0; q < s->its - H; ++q)
+                PS_CUDA(s, cudaMemcpyAsync(s->base[1 - s->cur] + (size_t)q * fe,
+                                           s->base[s->cur] + (size_t)(q + H) * fe,
+                                           fe * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        }
+        // algorithmic cell updates of each kernel in this half-cycle
+        double cP = 0, cY = 0, cG = 0, cO = 0;
+        for (int m = 1; m <= H; ++m) {
+            const double rp = s->bs - 2.0 * s->ops * m, rg = 2.0 * s->ops * m;
+            const double cs = (double)a.wy - 2.0 * s->ops * m, cm = 2.0 * s->ops * m;
+            cP += rp * cs;
+            cY += rp * cm;
+            cG += rg * cs;
+            cO += rg * cm;
+        }
+        const double u = (double)units;
+        if ((rc = timed_launch(s, 0, cP * u, [&] { K.P(a, units, stream_smem(s), s->stream); }))) return rc;
+        if ((rc = timed_launch(s, 1, cY * u, [&] { K.Y(a, units, seam_smem(s), s->stream); }))) return rc;
+        if ((rc = timed_launch(s, 2, cG * u, [&] { K.G(a, units, stream_smem(s), s->stream); }))) return rc;
+        if ((rc = timed_launch(s, 3, cO * u, [&] { K.O(a, units, seam_smem(s), s->stream); }))) return rc;
+        s->cur = 1 - s->cur;
+        off = ((off - a.hx) % s->nx + s->nx) % s->nx;
+        done += H;
+    }
+    return PS_OK;
+}
+
+int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t frame_cap,
+                 int frame_every)
+{
+    StdLaunch K = pick_standard(s->eq, s->ops);
+    if (!K) return fail(s, PS_ERR_UNSUPPORTED, "no standard kernel for equation %d", s->eq);
+    const size_t fe = field_elems(s);
+    for (int i = 0; i < 3; ++i)
+        if (!s->ring[i]) PS_CUDA(s, cudaMalloc(&s->ring[i], fe * sizeof(double)));
+    const int its = s->its;
+    // ring[c] = current level, ring[p] = previous level
+    int c = 0, p = 1, n = 2;
+    double* b = s->base[s->cur];
+    PS_CUDA(s, cudaMemcpyAsync(s->ring[c], b + (size_t)(its - 1) * fe, fe * sizeof(double),
+                               cudaMemcpyDeviceToDevice, s->stream));
+    PS_CUDA(s, cudaMemcpyAsync(s->ring[p], b + (size_t)(its >= 2 ? its - 2 : 0) * fe,
+                               fe * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    const EqParams prm = make_params(s);
+    const int every = frame_every > 0 ? frame_every : 1;
+    int rc;
+    for (int64_t L = 1; L <= nlevels; ++L) {
+        double* fr = nullptr;
+        if (frames && L % its == 0 && (L / its) % every == 0) {
+            const int64_t slot = (L / its) / every - 1;
+            if (slot < frame_cap) fr = frames + (size_t)slot * fe;
+        }
+        if ((rc = timed_launch(s, 4, (double)s->nx * s->ny, [&] {
+                 K(s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, s->nv,
+                   gts0 + (int)(L - 1), prm, s->stream);
+             })))
+            return rc;
+        const int t = p;
+        p = c;
+        c = n;
+        n = t;
+    }
+    // newest levels back into the base
+    PS_CUDA(s, cudaMemcpyAsync(b + (size_t)(its - 1) * fe, s->ring[c], fe * sizeof(double),
+                               cudaMemcpyDeviceToDevice, s->stream));
+    if (its >= 2)
+        PS_CUDA(s, cudaMemcpyAsync(b + (size_t)(its - 2) * fe, s->ring[p], fe * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, s->stream));
+    return PS_OK;
+}
+
+struct GlobalSpec {
+    const char* name;
+    int eqmask;  // bit per equation
+};
+
+const GlobalSpec kGlobals[] = {
+    {"DT", 0x1f},    {"DX", 0x1f},      {"DY", 0x1f},   {"ALPHA", 1 << PS_EQ_HEAT},
+    {"SCHEME", (1 << PS_EQ_HEAT) | (1 << PS_EQ_EXAMPLE) | (1 << PS_EQ_CHECKER)},
+    {"GAMMA", 1 << PS_EQ_EULER}, {"GAM_M1", 1 << PS_EQ_EULER}, {"DTDX", 1 << PS_EQ_EULER},
+    {"DTDY", 1 << PS_EQ_EULER},
+};
+
+const GlobalSpec* find_global(const ps_solver* s, const char* name)
+{
+    for (const auto& g : kGlobals)
+        if (!strcmp(g.name, name) && (g.eqmask >> s->eq & 1)) return &g;
+    return nullptr;
+}
+
+double decode_value(const void* value, size_t nbytes)
+{
+    switch (nbytes) {
+    case 8: {
+        double d;
+        memcpy(&d, value, 8);
+        return d;
+    }
+    case 4: {
+        int32_t i;
+        memcpy(&i, value, 4);
+        return (double)i;
+    }
+    case 2: {
+        int16_t i;
+        memcpy(&i, value, 2);
+        return (double)i;
+    }
+    case 1: return (double)*(const uint8_t*)value;
+    default: return 0.0;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ps_version(void) { return kVersion; }
+
+const char* ps_last_error(const ps_solver* s)
+{
+    return s ? s->err.c_str() : g_create_error.c_str();
+}
+
+int64_t ps_kernel_launches(const ps_solver* s) { return s ? s->launches : 0; }
+
+int ps_create(ps_solver** out, int device, int equation, int nv, int nx, int ny, int ops, int its,
+              int blocksize)
+{
+    if (!out) return PS_ERR_INVALID;
+    *out = nullptr;
+    if (equation < PS_EQ_HEAT || equation > PS_EQ_HALF) return PS_ERR_INVALID;
+    ps_solver* s = new ps_solver();
+    s->device = device;
+    s->eq = equation;
+    s->nv = nv;
+    s->nx = nx;
+    s->ny = ny;
+    s->ops = eq_ops(equation, ops);
+    s->its = its;
+    s->bs = blocksize;
+    int rc = PS_OK;
+    if (equation == PS_EQ_HEAT || equation == PS_EQ_HALF) {
+        if (nv != 1) rc = fail(s, PS_ERR_INVALID, "heat/half have one variable, got nv=%d", nv);
+    }
+    if (equation == PS_EQ_EULER && (nv != 4 || its != 2))
+        rc = fail(s, PS_ERR_INVALID, "euler needs nv=4 and its=2 (got nv=%d its=%d)", nv, its);
+    if (ops != s->ops) rc = fail(s, PS_ERR_INVALID, "equation %d has ops=%d, got %d", equation, s->ops, ops);
+    if (nv < 1 || nv > 4 || its < 1 || its > 2 || ops < 1 || ops > 2)
+        rc = fail(s, PS_ERR_UNSUPPORTED, "nv in 1..4, its in 1..2, ops in 1..2 supported");
+    if (blocksize <= 0 || blocksize % (2 * s->ops))  // io.py:52
+        rc = fail(s, PS_ERR_INVALID, "blocksize %d must be a multiple of 2*ops", blocksize);
+    if (rc == PS_OK && (nx % blocksize || ny % blocksize))  // process.py:143
+        rc = fail(s, PS_ERR_INVALID, "array %dx%d not divisible by blocksize %d", nx, ny, blocksize);
+    if (rc == PS_OK && (size_t)3 * nv * nx * ny >= (size_t)1 << 31)
+        rc = fail(s, PS_ERR_UNSUPPORTED, "field too large for 32-bit offsets");
+    s->mpss = blocksize / (2 * s->ops) - 1;
+    if (rc == PS_OK && s->mpss < 1)
+        rc = fail(s, PS_ERR_INVALID, "blocksize %d gives no swept level (MPSS < 1)", blocksize);
+    s->H = s->mpss;
+    s->chunk = (2 * s->ops * (s->H + 1) <= 32) ? 32 : 64;
+    s->nseg = 1;
+    if (rc == PS_OK) {
+        cudaError_t e = cudaSetDevice(device);
+        if (e != cudaSuccess) rc = fail(s, PS_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    }
+    if (rc == PS_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) rc = fail(s, PS_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        s->own_stream = true;
+    }
+    if (rc == PS_OK) {
+        const size_t bytes = (size_t)its * nv * nx * ny * sizeof(double);
+        for (int i = 0; i < 2 && rc == PS_OK; ++i) {
+            cudaError_t e = cudaMalloc(&s->base[i], bytes);
+            if (e != cudaSuccess) rc = fail(s, PS_ERR_NOMEM, "cudaMalloc base: %s", cudaGetErrorString(e));
+        }
+    }
+    if (rc != PS_OK) {
+        g_create_error = s->err;  // readable through ps_last_error(NULL)
+        ps_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return PS_OK;
+}
+
+int ps_destroy(ps_solver* s)
+{
+    if (!s) return PS_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto& b : s->base)
+        if (b) cudaFree(b);
+    for (auto& r : s->ring)
+        if (r) cudaFree(r);
+    if (s->xface) cudaFree(s->xface);
+    if (s->yface) cudaFree(s->yface);
+    for (auto& p : s->pending) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    for (auto e : s->event_pool) cudaEventDestroy(e);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return PS_OK;
+}
+
+int ps_set_global(ps_solver* s, const char* name, const void* value, size_t nbytes)
+{
+    if (!s || !name || !value) return PS_ERR_INVALID;
+    if (nbytes != 1 && nbytes != 2 && nbytes != 4 && nbytes != 8)
+        return fail(s, PS_ERR_INVALID, "constant %s: unsupported size %zu", name, nbytes);
+    if (!find_global(s, name)) return fail(s, PS_ERR_INVALID, "no constant named %s", name);
+    s->globals[name] = decode_value(value, nbytes);
+    return PS_OK;
+}
+
+int ps_get_global(ps_solver* s, const char* name, void** handle, size_t* size)
+{
+    if (!s || !name) return PS_ERR_INVALID;
+    const GlobalSpec* g = find_global(s, name);
+    if (!g) return fail(s, PS_ERR_INVALID, "no constant named %s", name);
+    if (handle) *handle = (void*)g;
+    if (size) *size = !strcmp(name, "SCHEME") ? 4 : 8;
+    return PS_OK;
+}
+
+int ps_set_global_handle(ps_solver* s, void* handle, const void* value, size_t nbytes)
+{
+    if (!s || !handle) return PS_ERR_INVALID;
+    return ps_set_global(s, ((const GlobalSpec*)handle)->name, value, nbytes);
+}
+
+int ps_get_global_value(ps_solver* s, const char* name, double* value)
+{
+    if (!s || !name || !value) return PS_ERR_INVALID;
+    const int SX = s->nx, SY = s->ny;
+    const int T = 2 * s->mpss + s->its;
+    if (!strcmp(name, "NV")) *value = s->nv;
+    else if (!strcmp(name, "SX")) *value = SX;
+    else if (!strcmp(name, "SY")) *value = SY;
+    else if (!strcmp(name, "VARS")) *value = (double)SX * SY;
+    else if (!strcmp(name, "TIMES")) *value = (double)s->nv * SX * SY;
+    else if (!strcmp(name, "MPSS")) *value = s->mpss;
+    else if (!strcmp(name, "MOSS")) *value = 2 * s->mpss;
+    else if (!strcmp(name, "OPS")) *value = s->ops;
+    else if (!strcmp(name, "ITS")) *value = s->its;
+    else if (!strcmp(name, "T")) *value = T;
+    else {
+        auto it = s->globals.find(name);
+        if (it == s->globals.end()) return fail(s, PS_ERR_INVALID, "no constant named %s", name);
+        *value = it->second;
+    }
+    return PS_OK;
+}
+
+int ps_configure(ps_solver* s, int h, int nseg, int chunk, int threads)
+{
+    if (!s) return PS_ERR_INVALID;
+    if (h < 0 || nseg < 0 || chunk < 0 || threads < 0) return fail(s, PS_ERR_INVALID, "negative knob");
+    if (h) {
+        if (h > s->mpss) return fail(s, PS_ERR_INVALID, "h %d > MPSS %d", h, s->mpss);
+        s->H = h;
+    }
+    if (nseg) s->nseg = nseg;
+    if (chunk) {
+        if (chunk != 32 && chunk != 64) return fail(s, PS_ERR_INVALID, "chunk must be 32 or 64");
+        s->chunk = chunk;
+    }
+    if (threads) {
+        if (threads != 256) return fail(s, PS_ERR_UNSUPPORTED, "threads must be 256");
+        s->threads = threads;
+    }
+    return PS_OK;
+}
+
+int ps_set_state(ps_solver* s, const double* src, int levels, int src_on_device)
+{
+    if (!s || !src) return PS_ERR_INVALID;
+    if (levels != 1 && levels != s->its)
+        return fail(s, PS_ERR_INVALID, "levels must be 1 or its=%d", s->its);
+    PS_CUDA(s, cudaSetDevice(s->device));
+    const size_t fe = field_elems(s);
+    const cudaMemcpyKind kind = src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int q = 0; q < s->its; ++q) {
+        const double* from = src + (size_t)(levels == 1 ? 0 : q) * fe;
+        PS_CUDA(s, cudaMemcpyAsync(s->base[s->cur] + (size_t)q * fe, from, fe * sizeof(double),
+                                   kind, s->stream));
+    }
+    if (!src_on_device) PS_CUDA(s, cudaStreamSynchronize(s->stream));
+    s->have_state = true;
+    return PS_OK;
+}
+
+int ps_run(ps_solver* s, int mode, int64_t nlevels, int gts0, double* frames, int64_t frame_cap,
+           int frame_every, int frames_on_device)
+{
+    if (!s) return PS_ERR_INVALID;
+    if (!s->have_state) return fail(s, PS_ERR_STATE, "ps_run before ps_set_state");
+    if (nlevels < 0) return fail(s, PS_ERR_INVALID, "negative level count");
+    if (frame_every < 0) return fail(s, PS_ERR_INVALID, "negative frame_every");
+    PS_CUDA(s, cudaSetDevice(s->device));
+    double* dframes = frames;
+    const size_t fe = field_elems(s);
+    if (frames && !frames_on_device) {
+        if (frame_cap > 0) PS_CUDA(s, cudaMallocAsync(&dframes, (size_t)frame_cap * fe * sizeof(double), s->stream));
+        else dframes = nullptr;
+    }
+    int rc;
+    if (mode == PS_MODE_SWEPT) rc = run_swept(s, nlevels, gts0, dframes, frame_cap, frame_every);
+    else if (mode == PS_MODE_STANDARD) rc = run_standard(s, nlevels, gts0, dframes, frame_cap, frame_every);
+    else rc = fail(s, PS_ERR_INVALID, "mode %d", mode);
+    if (frames && !frames_on_device && dframes) {
+        if (rc == PS_OK)
+            PS_CUDA(s, cudaMemcpyAsync(frames, dframes, (size_t)frame_cap * fe * sizeof(double),
+                                       cudaMemcpyDeviceToHost, s->stream));
+        cudaFreeAsync(dframes, s->stream);
+        PS_CUDA(s, cudaStreamSynchronize(s->stream));
+    }
+    return rc;
+}
+
+int ps_get_state(ps_solver* s, double* dst, int level, int dst_on_device)
+{
+    if (!s || !dst) return PS_ERR_INVALID;
+    if (level < 0 || level >= s->its) return fail(s, PS_ERR_INVALID, "level %d not in [0, its)", level);
+    PS_CUDA(s, cudaSetDevice(s->device));
+    const size_t fe = field_elems(s);
+    PS_CUDA(s, cudaMemcpyAsync(dst, s->base[s->cur] + (size_t)(s->its - 1 - level) * fe,
+                               fe * sizeof(double),
+                               dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               s->stream));
+    if (!dst_on_device) PS_CUDA(s, cudaStreamSynchronize(s->stream));
+    return PS_OK;
+}
+
+int ps_synchronize(ps_solver* s)
+{
+    if (!s) return PS_ERR_INVALID;
+    PS_CUDA(s, cudaSetDevice(s->device));
+    PS_CUDA(s, cudaStreamSynchronize(s->stream));
+    return drain_profile(s);
+}
+
+int ps_profile(ps_solver* s, int enable)
+{
+    if (!s) return PS_ERR_INVALID;
+    int rc = ps_synchronize(s);
+    if (rc) return rc;
+    s->profile = enable != 0;
+    for (int i = 0; i < 8; ++i) {
+        s->prof_ms[i] = 0;
+        s->prof_n[i] = 0;
+        s->prof_cells[i] = 0;
+    }
+    return PS_OK;
+}
+
+int ps_profile_read(ps_solver* s, int kind, double* ms, int64_t* launches, double* cells)
+{
+    if (!s || kind < 0 || kind >= 8) return PS_ERR_INVALID;
+    int rc = ps_synchronize(s);
+    if (rc) return rc;
+    if (ms) *ms = s->prof_ms[kind];
+    if (launches) *launches = s->prof_n[kind];
+    if (cells) *cells = s->prof_cells[kind];
+    return PS_OK;
+}
+
+int ps_set_stream(ps_solver* s, void* stream)
+{
+    if (!s) return PS_ERR_INVALID;
+    if (s->own_stream && s->stream) {
+        cudaStreamSynchronize(s->stream);
+        cudaStreamDestroy(s->stream);
+    }
+    if (stream) {
+        s->stream = (cudaStream_t)stream;
+        s->own_stream = false;
+    } else {
+        PS_CUDA(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        s->own_stream = true;
+    }
+    return PS_OK;
+}
+
+}  // extern "C"

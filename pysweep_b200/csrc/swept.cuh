@@ -1,0 +1,403 @@
+// Swept space-time engine.
+//
+// The reference decomposes the periodic domain into bs x bs blocks and runs,
+// per half-cycle of MPSS levels, the phases UpPyramid -> YBridge -> (shift by
+// bs/2 rows) -> XBridge -> Octahedron -> YBridge -> ... -> DownPyramid
+// (pysweep/core/pysweep.cu:64-249, pysweep/core/functions.py:12-123).  After
+// UpPyramid + YBridge every row band of height bs holds a "prism": level m is
+// complete on rows [OPS*m, bs-OPS*m) of the band, for every column.  After
+// XBridge + the Octahedron's down half the gap between two prisms is filled
+// and levels 1..MPSS are complete everywhere; the Octahedron's up half starts
+// the next prisms on bands shifted by bs/2.
+//
+// This engine keeps that structure with blocks of Bx rows x Wy columns
+// (Bx = bs sets MPSS = Bx/(2*OPS)-1; Wy is a multiple of the chunk width W):
+//
+//  P  (prism)   UpPyramid of one block.  The block is streamed through shared
+//               memory in W-column chunks; chunk c computes, at level m, the
+//               parallelogram of columns [c*W-OPS*m, (c+1)*W-OPS*m), so only the
+//               last 2*OPS columns of every level ("carry") pass from one chunk
+//               to the next.  At the block's left/right column edges the level
+//               shrinks by OPS per level, exactly as an up pyramid does.
+//  Y  (seam)    YBridge centred on each block column edge: grows in y, shrinks
+//               in x, fed by the two neighbours' edge columns (y-faces).
+//  G  (gap)     XBridge of the band boundary: rows [hx-OPS*m, hx+OPS*m) around
+//               the boundary (hx = Bx/2), streamed like P; the rows it reads
+//               from the two prisms (x-faces) come from global memory.
+//  O  (seam)    The Octahedron's down half at each gap/column-edge corner:
+//               grows in both x and y.
+//  The next half-cycle's P phase on bands shifted by hx is the Octahedron's up
+//  half (and, in the last half-cycle, G + O form the DownPyramid).
+//
+// Between phases only these pass through global memory:
+//   * the base levels (the last ITS complete levels; ping-pong bin/bout),
+//   * x-faces: 2*OPS rows at the top and bottom of every prism level,
+//   * y-faces: 2*OPS columns at the left/right edge of every stream level.
+// Every cell of every level is computed exactly once, by exactly the same
+// per-cell function as the standard decomposition, so swept and standard
+// results are bit-identical.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "equations.cuh"
+
+namespace psb {
+
+struct SweptArgs {
+    const double* __restrict__ bin;  // [ITS][nv][nx][ny], index 0 = oldest level
+    double* __restrict__ bout;       // same layout, levels of the next half-cycle
+    double* __restrict__ xface;      // [nb][Hmax-1][2][nv][2*OPS][ny]
+    double* __restrict__ yface;      // [nb*nseg][2][Hmax-1][nv][Bx][2*OPS]
+    double* __restrict__ frames;     // optional [nframes][nv][nx][ny]
+    long long frame_cap;             // number of frame slots
+    int frame_every;                 // store every k-th full step
+    int nx, ny, nv, bx, hx;
+    int H;        // levels in this half-cycle (<= Hmax)
+    int Hmax;     // levels the face buffers were sized for
+    int nb;       // bands (nx / bx)
+    int nseg, wy, nchunks;
+    int off;      // first row of prism band 0 (prism bands: off + i*bx)
+    int its;
+    long long L0;  // global level index of this half-cycle's level 0
+    int gts_base;  // the step function sees globalTimeStep = gts_base + level
+    EqParams p;
+};
+
+__device__ __forceinline__ int wrap(int v, int n)
+{
+    v %= n;
+    return v < 0 ? v + n : v;
+}
+
+// Frame slot for global level L, or -1.
+__device__ __forceinline__ long long frame_slot(const SweptArgs& a, long long L)
+{
+    if (!a.frames || L <= 0 || (L % a.its) != 0) return -1;
+    long long step = L / a.its;
+    if (step % a.frame_every) return -1;
+    long long s = step / a.frame_every - 1;
+    return s < a.frame_cap ? s : -1;
+}
+
+// ---------------------------------------------------------------- stream ----
+// One CTA = one (band, segment) block.  GAP = false: prism (UpPyramid);
+// GAP = true: gap (XBridge) centred on the band's upper boundary row.
+template <class Eq, int ITS, int W, bool GAP, int NT>
+__global__ void __launch_bounds__(NT) stream_kernel(SweptArgs a)
+{
+    extern __shared__ double sm[];
+    constexpr int OPS = Eq::OPS, O2 = 2 * OPS, RS = W + O2, NSLOT = ITS + 1;
+    constexpr int RG = NT / W;  // row groups
+    const int nv = a.nv, BX = a.bx, H = a.H, hx = a.hx, nx = a.nx, ny = a.ny;
+    const int SL = nv * BX * RS;  // one level slot
+    const int CS = nv * BX * O2;  // one carry
+    double* slot = sm;
+    double* carry = sm + NSLOT * SL;
+    const int unit = blockIdx.x;
+    const int band = unit / a.nseg, seg = unit % a.nseg;
+    const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
+    const int s0 = seg * a.wy;
+    const int tid = threadIdx.x;
+    const int tk = tid % W, tr = tid / W;
+    const int HF = a.Hmax - 1;
+    Nbr nb;
+    nb.vs = BX * RS;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        nb.x[k] = (k - 2) * RS;
+        nb.y[k] = k - 2;
+    }
+
+    for (int c = 0; c < a.nchunks; ++c) {
+        const int cw = s0 + c * W;
+        const bool first = (c == 0), last = (c == a.nchunks - 1);
+        const int Wc = last ? a.wy - c * W : W;  // the last chunk may be narrower
+        const int RC = Wc + O2;                  // columns of this chunk's level slots
+        // ---- level 0 and level -1 from the base --------------------------
+        {
+            const int lo0 = GAP ? hx - O2 : 0, hi0 = GAP ? hx + O2 : BX;
+            double* s0p = slot;  // slot of level 0
+            const double* b0 = a.bin + (size_t)(ITS - 1) * nv * nx * ny;
+            const int n0 = nv * (hi0 - lo0) * RC;
+            for (int e = tid; e < n0; e += NT) {
+                const int k = e % RC, t = e / RC;
+                const int i = lo0 + t % (hi0 - lo0), v = t / (hi0 - lo0);
+                const int g = wrap(cw - O2 + k, ny), r = wrap(r0 + i, nx);
+                s0p[(v * BX + i) * RS + k] = b0[((size_t)v * nx + r) * ny + g];
+            }
+            if (ITS >= 2) {
+                const int lo1 = GAP ? hx - OPS : OPS, hi1 = GAP ? hx + OPS : BX - OPS;
+                double* s1p = slot + (NSLOT - 1) * SL;  // slot of level -1
+                const double* b1 = a.bin + (size_t)(ITS - 2) * nv * nx * ny;
+                const int n1 = nv * (hi1 - lo1) * Wc;
+                for (int e = tid; e < n1; e += NT) {
+                    const int k = e % Wc, t = e / Wc;
+                    const int i = lo1 + t % (hi1 - lo1), v = t / (hi1 - lo1);
+                    const int g = wrap(cw - OPS + k, ny), r = wrap(r0 + i, nx);
+                    s1p[(v * BX + i) * RS + k] = b1[((size_t)v * nx + r) * ny + g];
+                }
+            }
+        }
+        __syncthreads();
+
+        for (int m = 1; m <= H; ++m) {
+            const int rlo = GAP ? hx - OPS * m : OPS * m;
+            const int rhi = GAP ? hx + OPS * m : BX - OPS * m;
+            const int klo = first ? O2 * (m + 1) : O2;
+            double* out = slot + (m % NSLOT) * SL;
+            const double* cur = slot + ((m - 1) % NSLOT) * SL;
+            const double* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
+            const int gts = a.gts_base + (int)(a.L0 + m);
+            // compute level m
+            {
+                const int k = O2 + tk;
+                if (k >= klo && k < RC) {
+                    for (int i = rlo + tr; i < rhi; i += RG) {
+                        const int o = i * RS + k;
+                        Eq::step(cur + o - OPS, prv + o - O2, out + o, nb, gts, nv, a.p);
+                    }
+                }
+            }
+            // carry in (previous chunk's last 2*OPS columns of level m)
+            if (!first) {
+                const double* cin = carry + m * CS;
+                for (int e = tid; e < CS; e += NT) {
+                    const int j = e % O2, t = e / O2;  // t = v*BX + i
+                    out[t * RS + j] = cin[e];
+                }
+            }
+            // carry out of level m-1
+            if (m - 1 >= 1) {
+                double* cout_ = carry + (m - 1) * CS;
+                for (int e = tid; e < CS; e += NT) {
+                    const int j = e % O2, t = e / O2;
+                    cout_[e] = cur[t * RS + W + j];
+                }
+            }
+            // gap: the prisms' rows of level m that the next level reads
+            if (GAP && m <= H - 1) {
+                const int nrow = 2 * O2;  // top band's bottom face + bottom band's top face
+                const int n = nv * nrow * Wc;
+                const int bup = wrap(band - 1, a.nb), bdn = band;
+                for (int e = tid; e < n; e += NT) {
+                    const int k = O2 + e % Wc, t = e / Wc;
+                    const int rr = t % nrow, v = t / nrow;
+                    const int side = rr < O2 ? 1 : 0;      // 1 = bottom face of upper band
+                    const int j = rr < O2 ? rr : rr - O2;
+                    const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
+                    const int bb = rr < O2 ? bup : bdn;
+                    const int g = wrap(cw - OPS * m - O2 + k, ny);
+                    const size_t fo =
+                        ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                    out[(v * BX + i) * RS + k] = a.xface[fo * ny + g];
+                }
+            }
+            __syncthreads();
+            // ---- outputs of level m --------------------------------------
+            {
+                const long long L = a.L0 + m;
+                const int ncol = RC - klo;
+                // x-faces (prism only)
+                if (!GAP && m <= H - 1) {
+                    const int n = nv * 2 * O2 * ncol;
+                    for (int e = tid; e < n; e += NT) {
+                        const int k = klo + e % ncol, t = e / ncol;
+                        const int rr = t % (2 * O2), v = t / (2 * O2);
+                        const int side = rr < O2 ? 0 : 1;  // 0 = top face, 1 = bottom face
+                        const int j = rr < O2 ? rr : rr - O2;
+                        const int i = side == 0 ? OPS * m + j : BX - OPS * m - O2 + j;
+                        const int g = wrap(cw - OPS * m - O2 + k, ny);
+                        const size_t fo =
+                            ((((size_t)band * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                        a.xface[fo * ny + g] = out[(v * BX + i) * RS + k];
+                    }
+                }
+                // base levels of the next half-cycle and frames
+                const bool tob = m > H - ITS;
+                const long long fs = frame_slot(a, L);
+                if (tob || fs >= 0) {
+                    const int nr = rhi - rlo;
+                    const int n = nv * nr * ncol;
+                    double* bo = tob ? a.bout + (size_t)(m - (H - ITS) - 1) * nv * nx * ny : nullptr;
+                    double* fr = fs >= 0 ? a.frames + (size_t)fs * nv * nx * ny : nullptr;
+                    for (int e = tid; e < n; e += NT) {
+                        const int k = klo + e % ncol, t = e / ncol;
+                        const int i = rlo + t % nr, v = t / nr;
+                        const int g = wrap(cw - OPS * m - O2 + k, ny), r = wrap(r0 + i, nx);
+                        const double val = out[(v * BX + i) * RS + k];
+                        const size_t go = ((size_t)v * nx + r) * ny + g;
+                        if (bo) bo[go] = val;
+                        if (fr) fr[go] = val;
+                    }
+                }
+                // y-faces at the block's column edges
+                if (m <= H - 1 && (first || last)) {
+                    const int nr = rhi - rlo;
+                    const int n = nv * nr * O2;
+                    for (int side = 0; side < 2; ++side) {
+                        if ((side == 0 && !first) || (side == 1 && !last)) continue;
+                        const int kb = side == 0 ? O2 * (m + 1) : Wc;
+                        double* yf = a.yface +
+                                     ((((size_t)unit * 2 + side) * HF + (m - 1)) * nv) * BX * O2;
+                        for (int e = tid; e < n; e += NT) {
+                            const int j = e % O2, t = e / O2;
+                            const int i = rlo + t % nr, v = t / nr;
+                            yf[(v * BX + i) * O2 + j] = out[(v * BX + i) * RS + kb + j];
+                        }
+                    }
+                }
+            }
+        }
+        // carry out of level H, then free the slots for the next chunk
+        if (!last) {
+            const double* cur = slot + (H % NSLOT) * SL;
+            double* cout_ = carry + H * CS;
+            for (int e = tid; e < CS; e += NT) {
+                const int j = e % O2, t = e / O2;
+                cout_[e] = cur[t * RS + W + j];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ seam ----
+// One CTA per (band, segment): the column edge at x0 = seg*wy between segment
+// seg-1 (left) and seg (right).  GAP = false: YBridge; GAP = true: the
+// Octahedron's down half.  Tile columns k <-> global x0 - KC + k, KC = OPS*(Hmax+1).
+template <class Eq, int ITS, bool GAP, int NT>
+__global__ void __launch_bounds__(NT) seam_kernel(SweptArgs a)
+{
+    extern __shared__ double sm[];
+    constexpr int OPS = Eq::OPS, O2 = 2 * OPS, NSLOT = ITS + 1;
+    const int nv = a.nv, BX = a.bx, H = a.H, hx = a.hx, nx = a.nx, ny = a.ny;
+    const int KC = OPS * (a.Hmax + 1);
+    const int TW = 2 * KC;
+    const int SL = nv * BX * TW;
+    double* slot = sm;
+    const int unit = blockIdx.x;
+    const int band = unit / a.nseg, seg = unit % a.nseg;
+    const int x0 = seg * a.wy;
+    const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
+    const int ul = band * a.nseg + (seg + a.nseg - 1) % a.nseg;  // left stream unit
+    const int ur = unit;                                          // right stream unit
+    const int tid = threadIdx.x;
+    const int HF = a.Hmax - 1;
+    Nbr nb;
+    nb.vs = BX * TW;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        nb.x[k] = (k - 2) * TW;
+        nb.y[k] = k - 2;
+    }
+    // level 0 (columns [KC-2OPS, KC+2OPS)) and level -1 (columns [KC-OPS, KC+OPS))
+    {
+        const int lo0 = GAP ? hx - O2 : 0, hi0 = GAP ? hx + O2 : BX;
+        const double* b0 = a.bin + (size_t)(ITS - 1) * nv * nx * ny;
+        const int nr = hi0 - lo0, n = nv * nr * 2 * O2;
+        for (int e = tid; e < n; e += NT) {
+            const int k = KC - O2 + e % (2 * O2), t = e / (2 * O2);
+            const int i = lo0 + t % nr, v = t / nr;
+            slot[(v * BX + i) * TW + k] =
+                b0[((size_t)v * nx + wrap(r0 + i, nx)) * ny + wrap(x0 - KC + k, ny)];
+        }
+        if (ITS >= 2) {
+            const int lo1 = GAP ? hx - OPS : OPS, hi1 = GAP ? hx + OPS : BX - OPS;
+            const double* b1 = a.bin + (size_t)(ITS - 2) * nv * nx * ny;
+            double* s1p = slot + (NSLOT - 1) * SL;
+            const int nr1 = hi1 - lo1, n1 = nv * nr1 * O2;
+            for (int e = tid; e < n1; e += NT) {
+                const int k = KC - OPS + e % O2, t = e / O2;
+                const int i = lo1 + t % nr1, v = t / nr1;
+                s1p[(v * BX + i) * TW + k] =
+                    b1[((size_t)v * nx + wrap(r0 + i, nx)) * ny + wrap(x0 - KC + k, ny)];
+            }
+        }
+    }
+    __syncthreads();
+    for (int m = 1; m <= H; ++m) {
+        const int rlo = GAP ? hx - OPS * m : OPS * m;
+        const int rhi = GAP ? hx + OPS * m : BX - OPS * m;
+        const int clo = KC - OPS * m, chi = KC + OPS * m;
+        double* out = slot + (m % NSLOT) * SL;
+        const double* cur = slot + ((m - 1) % NSLOT) * SL;
+        const double* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
+        const int gts = a.gts_base + (int)(a.L0 + m);
+        {
+            const int nc = chi - clo, nr = rhi - rlo;
+            for (int e = tid; e < nr * nc; e += NT) {
+                const int k = clo + e % nc, i = rlo + e / nc;
+                const int o = i * TW + k;
+                Eq::step(cur + o, prv + o, out + o, nb, gts, nv, a.p);
+            }
+        }
+        if (m <= H - 1) {
+            // y-faces of level m: left part from the left block's right edge,
+            // right part from the right block's left edge.
+            const int nr = rhi - rlo, n = nv * nr * O2;
+            const double* yl = a.yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
+            const double* yr = a.yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
+            for (int e = tid; e < n; e += NT) {
+                const int j = e % O2, t = e / O2;
+                const int i = rlo + t % nr, v = t / nr;
+                out[(v * BX + i) * TW + clo - O2 + j] = yl[(v * BX + i) * O2 + j];
+                out[(v * BX + i) * TW + chi + j] = yr[(v * BX + i) * O2 + j];
+            }
+            if (GAP) {
+                // the prisms' rows around the gap, columns [clo-2OPS, chi+2OPS)
+                const int nc = chi - clo + 2 * O2;
+                const int n2 = nv * 2 * O2 * nc;
+                const int bup = wrap(band - 1, a.nb), bdn = band;
+                for (int e = tid; e < n2; e += NT) {
+                    const int k = clo - O2 + e % nc, t = e / nc;
+                    const int rr = t % (2 * O2), v = t / (2 * O2);
+                    const int side = rr < O2 ? 1 : 0;
+                    const int j = rr < O2 ? rr : rr - O2;
+                    const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
+                    const int bb = rr < O2 ? bup : bdn;
+                    const size_t fo =
+                        ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                    out[(v * BX + i) * TW + k] = a.xface[fo * ny + wrap(x0 - KC + k, ny)];
+                }
+            }
+        }
+        __syncthreads();
+        // outputs of level m
+        {
+            const long long L = a.L0 + m;
+            const int nc = chi - clo;
+            if (!GAP && m <= H - 1) {
+                const int n = nv * 2 * O2 * nc;
+                for (int e = tid; e < n; e += NT) {
+                    const int k = clo + e % nc, t = e / nc;
+                    const int rr = t % (2 * O2), v = t / (2 * O2);
+                    const int side = rr < O2 ? 0 : 1;
+                    const int j = rr < O2 ? rr : rr - O2;
+                    const int i = side == 0 ? OPS * m + j : BX - OPS * m - O2 + j;
+                    const size_t fo =
+                        ((((size_t)band * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                    a.xface[fo * ny + wrap(x0 - KC + k, ny)] = out[(v * BX + i) * TW + k];
+                }
+            }
+            const bool tob = m > H - ITS;
+            const long long fs = frame_slot(a, L);
+            if (tob || fs >= 0) {
+                const int nr = rhi - rlo, n = nv * nr * nc;
+                double* bo = tob ? a.bout + (size_t)(m - (H - ITS) - 1) * nv * nx * ny : nullptr;
+                double* fr = fs >= 0 ? a.frames + (size_t)fs * nv * nx * ny : nullptr;
+                for (int e = tid; e < n; e += NT) {
+                    const int k = clo + e % nc, t = e / nc;
+                    const int i = rlo + t % nr, v = t / nr;
+                    const double val = out[(v * BX + i) * TW + k];
+                    const size_t go =
+                        ((size_t)v * nx + wrap(r0 + i, nx)) * ny + wrap(x0 - KC + k, ny);
+                    if (bo) bo[go] = val;
+                    if (fr) fr[go] = val;
+                }
+            }
+        }
+    }
+}
+
+}  // namespace psb

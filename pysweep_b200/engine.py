@@ -1,0 +1,172 @@
+"""Python handle on one device solver (a thin layer over the C ABI).
+
+``Engine`` owns a ``ps_solver``: the device copy of one periodic field, the
+buffers of the swept and standard decompositions, and a CUDA stream.  Host
+arrays are numpy ``float64``; device arrays may be given as torch CUDA tensors
+(their ``data_ptr`` is passed straight to the library).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import EQ, MODE, check
+
+DEFAULT_OPS = {"heat": 1, "half": 1, "euler": 2}
+DEFAULT_NV = {"heat": 1, "half": 1, "euler": 4}
+
+
+def _is_torch_cuda(x):
+    return hasattr(x, "is_cuda") and hasattr(x, "data_ptr") and x.is_cuda
+
+
+class Engine:
+    def __init__(self, equation, nx, ny, nv=None, ops=None, its=1, blocksize=16, device=0):
+        if equation not in EQ:
+            raise ValueError(f"unknown equation {equation!r}; built-ins are {sorted(EQ)}")
+        self.equation = equation
+        self.nv = nv if nv is not None else DEFAULT_NV.get(equation, 1)
+        self.ops = ops if ops is not None else DEFAULT_OPS.get(equation, 1)
+        self.nx, self.ny, self.its, self.bs, self.device = nx, ny, its, blocksize, device
+        self._h = ctypes.c_void_p()
+        L = _lib.lib()
+        rc = L.ps_create(ctypes.byref(self._h), device, EQ[equation], self.nv, nx, ny, self.ops,
+                         its, blocksize)
+        _lib.check(rc, None)
+        self.shape = (self.nv, nx, ny)
+
+    # -- constants ---------------------------------------------------------
+    def set_global(self, name, value):
+        """Set one plugin constant, typed like the value (float, int or bool)."""
+        if isinstance(value, (bool, np.bool_)):
+            buf, n = ctypes.c_uint8(int(value)), 1
+        elif isinstance(value, (int, np.integer)):
+            buf, n = ctypes.c_int32(int(value)), 4
+        else:
+            buf, n = ctypes.c_double(float(value)), 8
+        check(_lib.lib().ps_set_global(self._h, name.encode(), ctypes.byref(buf), n), self._h)
+
+    def get_global(self, name):
+        v = ctypes.c_double()
+        check(_lib.lib().ps_get_global_value(self._h, name.encode(), ctypes.byref(v)), self._h)
+        return v.value
+
+    def global_handle(self, name):
+        h = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        check(_lib.lib().ps_get_global(self._h, name.encode(), ctypes.byref(h), ctypes.byref(n)),
+              self._h)
+        return h.value, n.value
+
+    def set_global_handle(self, handle, raw: bytes):
+        buf = ctypes.create_string_buffer(raw, len(raw))
+        check(_lib.lib().ps_set_global_handle(self._h, ctypes.c_void_p(handle), buf, len(raw)),
+              self._h)
+
+    def configure(self, h=0, nseg=0, chunk=0, threads=0):
+        check(_lib.lib().ps_configure(self._h, h, nseg, chunk, threads), self._h)
+
+    # -- state -------------------------------------------------------------
+    def set_state(self, field):
+        """Initial levels: one field (copied to every base level) or `its` fields."""
+        if _is_torch_cuda(field):
+            levels = field.numel() // (self.nv * self.nx * self.ny)
+            check(_lib.lib().ps_set_state(self._h, ctypes.c_void_p(field.data_ptr()), levels, 1),
+                  self._h)
+            return
+        a = np.ascontiguousarray(field, dtype=np.float64)
+        levels = a.size // (self.nv * self.nx * self.ny)
+        check(_lib.lib().ps_set_state(self._h, a.ctypes.data_as(ctypes.c_void_p), levels, 0),
+              self._h)
+
+    def get_state(self, level=0, out=None):
+        if out is not None and _is_torch_cuda(out):
+            check(_lib.lib().ps_get_state(self._h, ctypes.c_void_p(out.data_ptr()), level, 1),
+                  self._h)
+            return out
+        a = out if out is not None else np.empty(self.shape)
+        check(_lib.lib().ps_get_state(self._h, a.ctypes.data_as(ctypes.c_void_p), level, 0),
+              self._h)
+        return a
+
+    def run(self, nlevels, mode="swept", gts0=1, frames=None, frame_every=1):
+        """Advance `nlevels` levels.  frames: None, a host array or a device tensor of
+        shape (k, nv, nx, ny) receiving every `frame_every`-th full step."""
+        if frames is None:
+            rc = _lib.lib().ps_run(self._h, MODE[mode], int(nlevels), gts0, None, 0, frame_every, 0)
+        elif _is_torch_cuda(frames):
+            rc = _lib.lib().ps_run(self._h, MODE[mode], int(nlevels), gts0,
+                                   ctypes.c_void_p(frames.data_ptr()), frames.shape[0],
+                                   frame_every, 1)
+        else:
+            assert frames.dtype == np.float64 and frames.flags.c_contiguous
+            rc = _lib.lib().ps_run(self._h, MODE[mode], int(nlevels), gts0,
+                                   frames.ctypes.data_as(ctypes.c_void_p), frames.shape[0],
+                                   frame_every, 0)
+        check(rc, self._h)
+
+    def synchronize(self):
+        check(_lib.lib().ps_synchronize(self._h), self._h)
+
+    KINDS = ("prism", "ybridge", "gap", "octahedron", "standard")
+
+    def profile(self, enable=True):
+        """Bracket every following launch with CUDA events (resets the counters)."""
+        check(_lib.lib().ps_profile(self._h, int(enable)), self._h)
+
+    def profile_read(self):
+        """{kind: (device ms, launches, algorithmic cell updates)} since profile()."""
+        out = {}
+        for i, k in enumerate(self.KINDS):
+            ms, n, cells = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
+            check(_lib.lib().ps_profile_read(self._h, i, ctypes.byref(ms), ctypes.byref(n),
+                                             ctypes.byref(cells)), self._h)
+            out[k] = (ms.value, n.value, cells.value)
+        return out
+
+    def set_stream(self, stream_handle):
+        check(_lib.lib().ps_set_stream(self._h, ctypes.c_void_p(stream_handle)), self._h)
+
+    @property
+    def launches(self):
+        return int(_lib.lib().ps_kernel_launches(self._h))
+
+    def close(self):
+        if self._h:
+            _lib.lib().ps_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def plugin_constants(equation, globals_):
+    """The constants a plugin's set_globals copies to the device
+    (pysweep/equations/heat.py:38-46, euler.py:25-31, example.py:40-48,
+    checker.py:37-45, half.py:35-39)."""
+    g = list(globals_)
+    if equation == "heat":
+        t0, tf, dt, dx, dy, alpha, scheme = g
+        return {"DT": float(dt), "DX": float(dx), "DY": float(dy), "ALPHA": float(alpha),
+                "SCHEME": bool(scheme)}
+    if equation == "euler":
+        t0, tf, dt, dx, dy, gamma = g
+        return {"DT": float(dt), "DX": float(dx), "DY": float(dy), "GAMMA": float(gamma),
+                "GAM_M1": float(gamma) - 1, "DTDX": float(dt) / float(dx),
+                "DTDY": float(dt) / float(dy)}
+    if equation in ("example", "checker"):
+        t0, tf, dt, dx, dy, scheme = g
+        return {"DT": float(dt), "DX": float(dx), "DY": float(dy), "SCHEME": bool(scheme)}
+    if equation == "half":
+        t0, tf, dt, dx, dy = g[:5]
+        return {"DT": float(dt), "DX": float(dx), "DY": float(dy)}
+    raise ValueError(equation)

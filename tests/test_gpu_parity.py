@@ -1,0 +1,149 @@
+"""GPU parity: the CUDA swept and standard paths against the reference's own
+frames (golden fixtures) and the CPU oracle.
+
+Bar: heat, half, example and checker are bitwise equal to the reference's
+numpy path.  Euler computes x**2 as x*x where numpy calls libm pow(), so the
+Euler frames are bitwise equal to the oracle run with x*x and within a
+relative max-norm of 1e-12 of the reference's own frames.  Swept and standard
+GPU results are always bit-identical.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+EULER_RTOL = 1e-12
+
+
+def _engine(eqn, shape, ops, its, bs, g):
+    from pysweep_b200 import Engine, plugin_constants
+    e = Engine(eqn, shape[1], shape[2], nv=shape[0], ops=ops, its=its, blocksize=bs)
+    for k, v in plugin_constants(eqn, g).items():
+        e.set_global(k, v)
+    return e
+
+
+def _gpu_frames(eqn, ic, g, ops, its, bs, nlevels, mode, **cfg):
+    e = _engine(eqn, ic.shape, ops, its, bs, g)
+    if cfg:
+        e.configure(**cfg)
+    e.set_state(ic)
+    nfr = nlevels // its
+    frames = np.zeros((nfr,) + ic.shape)
+    e.run(nlevels, mode=mode, frames=frames)
+    final = e.get_state()
+    e.close()
+    return np.concatenate([ic[None], frames]), final
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+@pytest.mark.parametrize("mode", ["swept", "standard"])
+def test_golden_frames(path, mode):
+    d = np.load(path)
+    eqn, ic, g = str(d["eqn"]), d["ic"], list(d["globals"])
+    ops, its, bs = int(d["ops"]), int(d["its"]), int(d["bs"])
+    ref = d[mode]
+    nlevels = (len(ref) - 1) * its
+    got, _ = _gpu_frames(eqn, ic, g, ops, its, bs, nlevels, mode)
+    assert got.shape == ref.shape
+    if eqn == "euler":
+        assert _rel(got, ref) < EULER_RTOL
+        mul, _, _ = oracle.standard(eqn, ic, g, its, nlevels, euler_square="mul")
+        assert np.array_equal(got, mul[: len(got)])
+    else:
+        assert np.array_equal(got, ref)
+
+
+CONFIGS = [
+    # eqn, n, bs, ops, its, steps, scheme, tiling
+    ("heat", 64, 8, 1, 1, 40, True, {}),
+    ("heat", 96, 16, 1, 1, 50, True, {"nseg": 3}),
+    ("heat", 128, 32, 1, 1, 61, True, {}),
+    ("heat", 128, 32, 1, 1, 61, True, {"h": 9, "nseg": 2}),
+    ("heat", 128, 64, 1, 1, 70, True, {}),
+    ("heat", 128, 16, 1, 2, 33, False, {"h": 4}),
+    ("heat", 96, 24, 1, 2, 25, False, {"nseg": 2}),
+    ("heat", 80, 8, 1, 1, 17, True, {"chunk": 64}),
+    ("euler", 64, 16, 2, 2, 12, None, {}),
+    ("euler", 64, 32, 2, 2, 10, None, {"nseg": 2}),
+    ("euler", 96, 16, 2, 2, 9, None, {"h": 2, "nseg": 3}),
+    ("half", 64, 16, 1, 2, 20, None, {}),
+    ("checker", 48, 8, 2, 2, 12, False, {}),
+    ("example", 48, 12, 1, 1, 21, True, {"nseg": 2}),
+]
+
+
+def _ic_and_globals(eqn, n, steps, scheme):
+    rng = np.random.default_rng(n * 7 + steps)
+    if eqn == "heat":
+        dx = 1.0 / n
+        dt = 0.2 * dx * dx
+        return rng.standard_normal((1, n, n)), [0, steps * dt, dt, dx, dx, 1.0, scheme]
+    if eqn == "euler":
+        x = np.linspace(-5, 5, n, endpoint=False)
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        r2 = X ** 2 + Y ** 2
+        rho = 1 - 0.3 * np.exp(-r2)
+        u = 1 + 0.2 * np.sin(2 * np.pi * Y / 10)
+        v = 1 - 0.2 * np.cos(2 * np.pi * X / 10)
+        p = 1 / 1.4 * (1 - 0.2 * np.exp(-r2))
+        E = p / 0.4 + 0.5 * rho * (u * u + v * v)
+        dx = 10.0 / n
+        return np.stack([rho, rho * u, rho * v, E]), [0, steps * 0.1 * dx, 0.1 * dx, dx, dx, 1.4]
+    if eqn == "half":
+        return rng.standard_normal((1, n, n)), [0, 1, 0.1, 0.1, 0.1]
+    return rng.integers(0, 2, (1, n, n)).astype(float), [0, 1, 0.1, 0.1, 0.1, scheme]
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=[f"{c[0]}-n{c[1]}-bs{c[2]}-its{c[4]}-{c[7]}" for c in CONFIGS])
+def test_swept_standard_oracle(cfg):
+    eqn, n, bs, ops, its, steps, scheme, tiling = cfg
+    ic, g = _ic_and_globals(eqn, n, steps, scheme)
+    nlevels = steps * its
+    sw, swf = _gpu_frames(eqn, ic, g, ops, its, bs, nlevels, "swept", **tiling)
+    st, stf = _gpu_frames(eqn, ic, g, ops, its, bs, nlevels, "standard")
+    assert np.array_equal(sw, st), "swept and standard differ"
+    assert np.array_equal(swf, stf)
+    ref, _, _ = oracle.standard(eqn, ic, g, its, nlevels,
+                                euler_square="mul" if eqn == "euler" else "pow")
+    assert np.array_equal(sw, ref[: len(sw)])
+
+
+def test_heat_384_reference_step_count_and_analytic():
+    """The 384^2 heat case: the reference's step rounding (497 steps for bs 16),
+    bitwise against the oracle's reference swept decomposition, and the analytic
+    decaying sine to truncation error."""
+    n, bs = 384, 16
+    dx = 1.0 / n
+    dt = 0.2 * dx * dx
+    g = [0, 500 * dt, dt, dx, dx, 1.0, True]
+    ts, mpss, mgss = oracle.step_data(g, bs, 1, 1)
+    nlevels = mpss * (mgss + 1)
+    assert nlevels == 497
+    x = np.arange(n) / n
+    ic = (np.sin(2 * np.pi * x)[:, None] * np.sin(2 * np.pi * x)[None, :])[None]
+    frames, final = _gpu_frames("heat", ic, g, 1, 1, bs, nlevels, "swept")
+    ref, _ = oracle.swept("heat", ic, g, 1, 1, bs, nthreads=oracle.max_threads())
+    assert np.array_equal(frames, ref)
+    exact = np.exp(-8 * np.pi ** 2 * nlevels * dt) * ic
+    assert np.abs(final - exact).max() < 1e-4
+
+
+def test_euler_mass_conserved_and_decompositions_agree_at_256():
+    n, steps = 256, 40
+    ic, g = _ic_and_globals("euler", n, steps, None)
+    sw, swf = _gpu_frames("euler", ic, g, 2, 2, 32, steps * 2, "swept", nseg=2)
+    st, stf = _gpu_frames("euler", ic, g, 2, 2, 32, steps * 2, "standard")
+    assert np.array_equal(swf, stf)
+    m0, m1 = ic[0].sum(), swf[0].sum()
+    assert abs(m1 - m0) / m0 < 1e-12
