@@ -86,7 +86,9 @@ int ps_get_global_value(ps_solver *s, const char *name, double *value);
 /*
  * Tiling knobs of the swept decomposition (0 keeps the current value):
  * h = levels per half-cycle (1..MPSS), nseg = column blocks per row band,
- * chunk = streaming chunk width (32 or 64), threads = threads per CTA.
+ * chunk = streaming chunk width (32 or 64) of the generic streams,
+ * threads = 128 (default: register-resident heat streams where they apply)
+ * or 256 (always the generic shared-memory streams).
  * The defaults reproduce the reference's MPSS with bs-row bands.
  */
 int ps_configure(ps_solver *s, int h, int nseg, int chunk, int threads);

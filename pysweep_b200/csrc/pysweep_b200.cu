@@ -6,12 +6,14 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/pysweep_b200.h"
 #include "equations.cuh"
 #include "swept.cuh"
+#include "heat_fast.cuh"
 
 namespace psb {
 
@@ -56,7 +58,7 @@ struct ps_solver {
     int nv = 1, nx = 0, ny = 0, ops = 1, its = 1, bs = 0;
     int mpss = 0;
     // tiling
-    int H = 0, nseg = 1, chunk = 32, threads = 256;
+    int H = 0, nseg = 1, chunk = 32, threads = 128;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     // named plugin constants
@@ -87,16 +89,21 @@ namespace {
 const char* kVersion = "pysweep_b200 0.1.0 (sm_100a)";
 thread_local std::string g_create_error;  // message of the last failed ps_create
 
-// Opt a kernel into the large dynamic shared-memory carve-out, once per device.
+// Opt a kernel into the large dynamic shared-memory carve-out, once per
+// (kernel, device).
+std::mutex g_attr_mu;
+std::map<std::pair<const void*, int>, bool> g_attr_done;
+
 template <class K>
 void allow_big_smem(K kernel)
 {
-    static unsigned done = 0;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 32 && !(done >> dev & 1u)) {
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    if (!g_attr_done[key]) {
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        done |= 1u << dev;
+        g_attr_done[key] = true;
     }
 }
 
@@ -197,7 +204,17 @@ void launch_standard(const double* cur, const double* prev, double* out, double*
 
 struct SweptSet {
     SweptLaunch P, Y, G, O;
+    bool fast = false;
 };
+
+template <int BX, bool GAP>
+void launch_fast(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
+{
+    auto k = heat_stream_fast<BX, GAP>;
+    allow_big_smem(k);
+    const int units = a.nb * a.nseg;
+    k<<<(units + kFastWarps - 1) / kFastWarps, 32 * kFastWarps, smem, st>>>(a);
+}
 
 template <class Eq, int ITS, int W>
 SweptSet make_set()
@@ -343,12 +360,30 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         return fail(s, PS_ERR_UNSUPPORTED, "no swept kernels for equation %d ops %d its %d chunk %d",
                     s->eq, s->ops, s->its, s->chunk);
     const int O2 = 2 * s->ops;
+    // register-resident streams for heat with forward Euler (the generic
+    // seam kernels are shared)
+    const bool fwd_euler = make_params(s).i[0] != 0;
+    if (s->eq == PS_EQ_HEAT && s->its == 1 && fwd_euler && s->threads != 256 &&
+        (s->bs == 16 || s->bs == 32) && s->ny % s->nseg == 0 &&
+        (s->ny / s->nseg) % kFastChunk == 0) {
+        K.fast = true;
+        if (s->bs == 16) {
+            K.P = launch_fast<16, false>;
+            K.G = launch_fast<16, true>;
+        } else {
+            K.P = launch_fast<32, false>;
+            K.G = launch_fast<32, true>;
+        }
+    }
     if (s->H < 1 || s->H > s->mpss) return fail(s, PS_ERR_INVALID, "levels per half-cycle %d not in [1, %d]", s->H, s->mpss);
     if (s->chunk < O2 * (s->H + 1))
         return fail(s, PS_ERR_INVALID, "chunk %d narrower than 2*ops*(h+1) = %d", s->chunk, O2 * (s->H + 1));
-    if (s->ny % s->nseg || (s->ny / s->nseg) % s->chunk)
-        return fail(s, PS_ERR_INVALID, "ny %d not divisible into %d segments of whole %d-column chunks",
-                    s->ny, s->nseg, s->chunk);
+    if (s->nseg < 1 || s->ny % s->nseg)
+        return fail(s, PS_ERR_INVALID, "ny %d not divisible into %d segments", s->ny, s->nseg);
+    // the first chunk of a segment shrinks by 2*ops per level on its left edge
+    if (std::min(s->chunk, s->ny / s->nseg) < O2 * (s->H + 1))
+        return fail(s, PS_ERR_INVALID, "segment width %d narrower than 2*ops*(h+1) = %d",
+                    s->ny / s->nseg, O2 * (s->H + 1));
     const size_t smem = std::max(stream_smem(s), seam_smem(s));
     if (smem > 227 * 1024)
         return fail(s, PS_ERR_UNSUPPORTED, "tile needs %zu bytes of shared memory", smem);
@@ -368,7 +403,9 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     a.nb = s->nx / s->bs;
     a.nseg = s->nseg;
     a.wy = s->ny / s->nseg;
-    a.nchunks = a.wy / s->chunk;
+    // the last chunk may be partial (generic streams); the register streams
+    // use whole 64-column chunks
+    a.nchunks = K.fast ? a.wy / kFastChunk : (a.wy + s->chunk - 1) / s->chunk;
     a.its = s->its;
     a.gts_base = gts0 - 1;
     a.xface = s->xface;
@@ -403,9 +440,11 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
             cO += rg * cm;
         }
         const double u = (double)units;
-        if ((rc = timed_launch(s, 0, cP * u, [&] { K.P(a, units, stream_smem(s), s->stream); }))) return rc;
+        const size_t psm = K.fast ? (s->bs == 16 ? heat_fast_smem<16>(s->H) : heat_fast_smem<32>(s->H))
+                                  : stream_smem(s);
+        if ((rc = timed_launch(s, 0, cP * u, [&] { K.P(a, units, psm, s->stream); }))) return rc;
         if ((rc = timed_launch(s, 1, cY * u, [&] { K.Y(a, units, seam_smem(s), s->stream); }))) return rc;
-        if ((rc = timed_launch(s, 2, cG * u, [&] { K.G(a, units, stream_smem(s), s->stream); }))) return rc;
+        if ((rc = timed_launch(s, 2, cG * u, [&] { K.G(a, units, psm, s->stream); }))) return rc;
         if ((rc = timed_launch(s, 3, cO * u, [&] { K.O(a, units, seam_smem(s), s->stream); }))) return rc;
         s->cur = 1 - s->cur;
         off = ((off - a.hx) % s->nx + s->nx) % s->nx;
@@ -658,7 +697,10 @@ int ps_configure(ps_solver* s, int h, int nseg, int chunk, int threads)
         s->chunk = chunk;
     }
     if (threads) {
-        if (threads != 256) return fail(s, PS_ERR_UNSUPPORTED, "threads must be 256");
+        // 128: register-resident heat streams where they apply (default);
+        // 256: always the generic shared-memory streams
+        if (threads != 256 && threads != 128)
+            return fail(s, PS_ERR_UNSUPPORTED, "threads must be 128 or 256");
         s->threads = threads;
     }
     return PS_OK;

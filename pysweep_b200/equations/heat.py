@@ -1,0 +1,31 @@
+"""Heat equation plugin: constants and analytic solution.
+
+Contract of pysweep/equations/heat.py:33-46 (set_globals: t0, tf, dt, dx, dy,
+alpha, scheme; device constants DT, DX, DY, ALPHA, SCHEME) and the decaying
+sine of heat.py:95-113.
+"""
+import numpy
+
+from pysweep_b200.solver import driver_shim as cuda
+
+scheme = True
+
+
+def set_globals(*args, source_mod=None):
+    global dt, dx, dy, alpha, scheme, courant
+    t0, tf, dt, dx, dy, alpha, scheme = args
+    courant = alpha * dt / dx / dx
+    if source_mod is not None:
+        for key, val in zip(("DT", "DX", "DY", "ALPHA"), args[2:6]):
+            ckey, _ = source_mod.get_global(key)
+            cuda.memcpy_htod(ckey, numpy.float64(val))
+        ckey, _ = source_mod.get_global("SCHEME")
+        cuda.memcpy_htod(ckey, numpy.intc(scheme))
+
+
+def analytical(npx, npy, t, alpha=0.1):
+    """sin(2 pi x) sin(2 pi y) exp(-8 pi^2 alpha t) on x_i = i/npx."""
+    X = numpy.linspace(0, 1, npx, endpoint=False)
+    Y = numpy.linspace(0, 1, npy, endpoint=False)
+    u = numpy.sin(2 * numpy.pi * X)[:, None] * numpy.sin(2 * numpy.pi * Y)[None, :]
+    return (u * numpy.exp(-8 * numpy.pi ** 2 * alpha * t))[None], X, Y

@@ -1,0 +1,319 @@
+"""Drop-in replacement for ``pysweep.Solver`` (pysweep/core/solver.py).
+
+    solver = pysweep_b200.Solver(initialConditions, "input.yaml")
+    solver()
+
+The yaml keys, their defaults and the attributes a script may set directly
+are those of pysweep/core/io.py:35-75 (``swept``, ``verbose``,
+``intermediate_steps``, ``operating_points``, ``blocksize``, ``share``,
+``exid``, ``globals``, ``cpu``, ``gpu``, ``filename``, ``dtype``).  The time
+step arithmetic is the reference's (solver.py:113-128): a swept run computes
+``MPSS*(maxGlobalSweptStep+1)`` levels and stores ``timeSteps`` frames, a
+standard run stores ``timeSteps+1`` frames.
+
+What runs where: every row runs on the GPU through the CUDA swept (or
+standard) kernels.  ``share`` below 1 requested a CPU/GPU split in the
+reference; the computed values do not depend on the decomposition (the
+reference's own swept, standard and CPU paths agree bitwise), so the whole
+domain runs on the GPU and the effective share is recorded as 1.0.
+
+The CPU plugin (``cpu:``) keeps its contract: its ``set_globals(*globals,
+source_mod=...)`` is called with a module object whose ``get_global(name)``
+and the ``cuda.memcpy_htod`` it uses set the device constants, exactly as
+with a PyCUDA SourceModule (pysweep/equations/heat.py:38-46).  The GPU hook
+(``gpu:``) names the step function: the file names of the reference's
+plugins (heat.cu, euler.cu, example.cu, checker.cu, half.cu) and the bare
+names select the built-in sm_100a kernels.
+
+Output: the reference's HDF5 layout (io.py:78-90): datasets ``blocksize``,
+``share``, ``exid``, ``globals``, ``clocktime`` and ``data[t, v, x, y]``.
+h5py is used when importable; otherwise the same datasets go to an ``.npz``
+file next to the requested name.  ``output_every`` (extra yaml key, default 1)
+keeps every k-th frame, ``write_output: false`` skips the file.
+"""
+import importlib.util
+import os
+import time
+import types
+import warnings
+from datetime import datetime
+
+import numpy as np
+import yaml
+
+from .engine import Engine, plugin_constants
+
+BUILTIN = ("heat", "euler", "example", "checker", "half")
+NV = {"heat": 1, "half": 1, "euler": 4}
+
+
+# ----------------------------------------------------- SourceModule stand-in
+class GlobalRef:
+    """What ``source_mod.get_global(name)[0]`` returns: a device constant."""
+
+    def __init__(self, module, name):
+        self.module, self.name = module, name
+
+
+class SourceModuleShim:
+    """Duck type of pycuda.compiler.SourceModule for the plugins' set_globals."""
+
+    def __init__(self):
+        self.values = {}
+        self.engine = None
+
+    def get_global(self, name):
+        size = 4 if name == "SCHEME" else 8
+        return GlobalRef(self, name), size
+
+    def apply(self, engine):
+        self.engine = engine
+        for k, v in self.values.items():
+            engine.set_global(k, v)
+
+
+def memcpy_htod(dst, src):
+    """pycuda.driver.memcpy_htod for GlobalRef destinations."""
+    if not isinstance(dst, GlobalRef):
+        raise TypeError("memcpy_htod: destination is not a pysweep_b200 constant")
+    if isinstance(src, (bytes, bytearray)):
+        val = int.from_bytes(bytes(src), "little") if src else 0
+    else:
+        a = np.asarray(src)
+        if a.dtype.kind == "f":
+            val = float(a)
+        elif a.dtype.kind == "b":
+            val = bool(a)
+        else:
+            val = int(a)
+    dst.module.values[dst.name] = val
+    if dst.module.engine is not None:
+        dst.module.engine.set_global(dst.name, val)
+
+
+driver_shim = types.SimpleNamespace(memcpy_htod=memcpy_htod)
+
+
+# ------------------------------------------------------------------ Solver
+class Solver:
+    def __init__(self, initialConditions=None, yamlFileName=None, sendWarning=True):
+        self.moments = [time.time()]
+        self.rank = 0
+        self.clusterMasterBool = True
+        self.nodeMasterBool = True
+        self.gpuBool = True
+        self.assignInitialConditions(initialConditions, sendWarning=sendWarning)
+        # defaults of io.yamlManager
+        self.simulation = True
+        self.verbose = False
+        self.intermediate = 1
+        self.operating = 1
+        self.blocksize = (32, 32, 1)
+        self.share = 0.9
+        self.exid = []
+        self.globals = []
+        self.cpu = self.cpuStr = ""
+        self.gpu = self.gpuStr = ""
+        self.output = "output.hdf5"
+        self.dtypeStr = "float64"
+        self.dtype = np.dtype("float64")
+        self.output_every = 1
+        self.write_output = True
+        self.device = 0
+        self.tiling = {}
+        if yamlFileName is not None:
+            self.yamlFileName = yamlFileName
+            self._read_yaml()
+        elif sendWarning:
+            warnings.warn("yaml not specified, requires manual input.")
+
+    # -- configuration -----------------------------------------------------
+    def _read_yaml(self):
+        with open(self.yamlFileName) as f:
+            y = yaml.load(f, Loader=yaml.FullLoader) or {}
+        get = lambda k, d: y[k] if k in y else d  # noqa: E731
+        self.simulation = get("swept", True)
+        self.verbose = get("verbose", False)
+        self.intermediate = get("intermediate_steps", 1)
+        self.operating = get("operating_points", 1)
+        bs = get("blocksize", 32)
+        assert bs % (2 * self.operating) == 0, (
+            "Invalid blocksize, blocksize must satisfy BS = 2*ops*k and the architectural "
+            "limit where k is any integer factor.")
+        self.blocksize = (bs, bs, 1)
+        self.share = get("share", 0.9)
+        self.exid = get("exid", [])
+        self.globals = get("globals", [])
+        self.cpuStr = self.cpu = get("cpu", "")
+        self.gpuStr = self.gpu = get("gpu", "")
+        self.output = get("filename", "output.hdf5")
+        self.dtypeStr = get("dtype", "float64")
+        self.dtype = np.dtype(self.dtypeStr)
+        self.output_every = int(get("output_every", 1))
+        self.write_output = bool(get("write_output", True))
+        self.tiling = get("tiling", {}) or {}
+        if self.cpu:
+            self.loadCPUModule()
+
+    def setGPU(self, gpu):
+        self.gpu = self.gpuStr = gpu
+
+    def setCPU(self, cpu):
+        self.cpu = self.cpuStr = cpu
+
+    def loadCPUModule(self):
+        """Import the CPU plugin from its path (solver.py:83-87)."""
+        if isinstance(self.cpu, types.ModuleType):
+            return
+        path = os.path.abspath(self.cpu)
+        spec = importlib.util.spec_from_file_location("module.step", path)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.cuda = driver_shim  # set_globals calls cuda.memcpy_htod
+        self.cpu = mod
+
+    def assignInitialConditions(self, initialConditions, sendWarning=True):
+        """An array (nv, nx, ny), or a file holding dataset ``data`` (solver.py:89-101)."""
+        if isinstance(initialConditions, str):
+            self.initialConditions = _read_data(initialConditions)
+            self.arrayShape = self.initialConditions.shape
+        elif initialConditions is not None:
+            self.initialConditions = np.asarray(initialConditions, dtype=np.float64)
+            self.arrayShape = self.initialConditions.shape
+        elif sendWarning:
+            warnings.warn("Initial condition not provided, requires manual assignment with "
+                          "assignInitialConditionsFunction.")
+
+    def equation(self):
+        name = os.path.splitext(os.path.basename(str(self.gpu)))[0]
+        if name not in BUILTIN:
+            raise NotImplementedError(
+                f"GPU hook {self.gpu!r}: built-in step functions are {BUILTIN}")
+        return name
+
+    def createTimeStepData(self):
+        """pysweep/core/solver.py:113-128."""
+        g = self.globals
+        self.timeSteps = int((g[1] - g[0]) / g[2])
+        if self.simulation:
+            self.maxPyramidSize = self.blocksize[0] // (2 * self.operating) - 1
+            self.maxGlobalSweptStep = int(self.intermediate * self.timeSteps / self.maxPyramidSize - 1)
+            self.timeSteps = int(self.maxPyramidSize * (self.maxGlobalSweptStep + 1) / self.intermediate + 1)
+            self.maxOctSize = 2 * self.maxPyramidSize
+            self.levels = self.maxPyramidSize * (self.maxGlobalSweptStep + 1)
+            self.nframes = self.timeSteps
+        else:
+            # standardSolve computes intermediate*(timeSteps+1) levels and stores
+            # levels 0..timeSteps (solver.py:185, io.py:189-193)
+            self.levels = self.intermediate * (self.timeSteps + 1)
+            self.nframes = self.timeSteps + 1
+
+    # -- run ---------------------------------------------------------------
+    def __call__(self, start=0, stop=-1):
+        self.moments.append(time.time())
+        if self.share < 1:
+            warnings.warn(f"share={self.share}: all rows run on the GPU (results do not depend "
+                          "on the CPU/GPU split)")
+        eqn = self.equation()
+        ic = np.asarray(self.initialConditions, dtype=np.float64)
+        if ic.ndim == 2:
+            ic = ic[None]
+        nv, nx, ny = ic.shape
+        self.createTimeStepData()
+        self.moments.append(time.time())
+        self.engine = Engine(eqn, nx, ny, nv=nv, ops=self.operating, its=self.intermediate,
+                             blocksize=self.blocksize[0], device=self.device)
+        if self.tiling:
+            self.engine.configure(**self.tiling)
+        src = SourceModuleShim()
+        if isinstance(self.cpu, types.ModuleType) and hasattr(self.cpu, "set_globals"):
+            self.cpu.set_globals(*self.globals, source_mod=src)
+            if not src.values:  # the plugin set only CPU globals
+                src.values = plugin_constants(eqn, self.globals)
+        else:
+            src.values = plugin_constants(eqn, self.globals)
+        src.apply(self.engine)
+        self.engine.set_state(ic)
+        self.moments.append(time.time())
+        every = max(1, self.output_every)
+        # frames beyond the initial condition at full steps 1..nframes-1
+        nkeep = (self.nframes - 1) // every
+        frames = np.empty((nkeep,) + ic.shape) if (self.write_output and nkeep) else None
+        mode = "swept" if self.simulation else "standard"
+        self.engine.run(self.levels, mode=mode, frames=frames, frame_every=every)
+        self.engine.synchronize()
+        self.moments.append(time.time())
+        self.final = self.engine.get_state()
+        if frames is not None:
+            self.data = np.concatenate([ic[None], frames])
+        else:
+            self.data = ic[None]
+        self.arrayShape = (self.nframes,) + ic.shape
+        if self.write_output:
+            self._write(self.data, self.moments[-1] - self.moments[0])
+        self.engine.close()
+        clock = self.moments[stop] - self.moments[start]
+        _update_log(self, clock)
+        if self.verbose:
+            print(f"Done in {self.moments[-1] - self.moments[0]} seconds...")
+
+    def _write(self, data, clocktime):
+        payload = {"blocksize": np.array([self.blocksize[0]]), "share": np.array([1.0]),
+                   "exid": np.array(self.exid), "globals": np.array(self.globals, dtype=float),
+                   "clocktime": np.array([clocktime]), "data": data.astype(self.dtype)}
+        try:
+            import h5py
+        except ImportError:
+            h5py = None
+        if h5py is not None:
+            with h5py.File(self.output, "w") as f:
+                for k, v in payload.items():
+                    f.create_dataset(k, data=v)
+        else:
+            base, _ = os.path.splitext(self.output)
+            np.savez(base + ".npz", **payload)
+
+    def __str__(self):
+        s = "\nPysweep simulation properties:\n"
+        s += f"\tsimulation type: {'swept' if self.simulation else 'standard'}\n"
+        s += f"\tgpu source: {self.gpuStr}\n\tcpu source: {self.cpuStr}\n"
+        s += f"\toutput file: {self.output}\n\tverbose: {self.verbose}\n"
+        s += f"\tArray shape: {getattr(self, 'arrayShape', None)}\n\tdtype: {self.dtype}\n"
+        s += f"\tshare: {self.share}\n\tblocksize: {self.blocksize[0]}\n"
+        s += f"\tstencil size: {int(self.operating * 2 + 1)}\n"
+        s += f"\tintermediate time steps: {self.intermediate}\n"
+        if self.globals:
+            s += "\ttime data (t0,tf,dt): ({},{},{})\n".format(*self.globals[:3])
+        return s
+
+    def compactPrint(self):
+        moment = self.moments[-1] - self.moments[0] if self.moments else None
+        print(("swept: " if self.simulation else "standard: ") +
+              f"{self.blocksize[0]}, {self.share}, {self.intermediate}, {self.operating}, "
+              f"{getattr(self, 'timeSteps', None)}, {moment}")
+
+
+def _read_data(path):
+    if path.endswith(".npy"):
+        return np.load(path)
+    if path.endswith(".npz"):
+        return np.load(path)["data"]
+    import h5py  # noqa: WPS433 - only HDF5 inputs need it
+    with h5py.File(path, "r") as f:
+        return np.array(f["data"])
+
+
+def _update_log(solver, clocktime, path="log.yaml"):
+    """Append the run to ./log.yaml with the reference's keys (io.py:10-27)."""
+    entry = {datetime.now().strftime("%m/%d/%Y-%H:%M:%S"): {
+        "runtime": float(clocktime), "swept": bool(solver.simulation),
+        "blocksize": int(solver.blocksize[0]), "share": 1.0, "cpu": str(solver.cpuStr),
+        "array_shape": [int(x) for x in solver.arrayShape],
+        "time_per_step": float(clocktime / max(solver.arrayShape[0] - 1, 1))}}
+    prev = {}
+    if os.path.isfile(path):
+        with open(path) as f:
+            prev = yaml.load(f, Loader=yaml.FullLoader) or {}
+    prev.update(entry)
+    with open(path, "w") as f:
+        yaml.dump(prev, f)

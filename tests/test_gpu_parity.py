@@ -147,3 +147,29 @@ def test_euler_mass_conserved_and_decompositions_agree_at_256():
     assert np.array_equal(swf, stf)
     m0, m1 = ic[0].sum(), swf[0].sum()
     assert abs(m1 - m0) / m0 < 1e-12
+
+
+FAST = [
+    # n, bs, steps, tiling
+    (128, 32, 45, {}),
+    (128, 32, 40, {"nseg": 2}),
+    (192, 16, 33, {}),
+    (256, 16, 29, {"nseg": 4, "h": 5}),
+    (128, 32, 20, {"h": 4}),
+    (64, 32, 31, {}),
+]
+
+
+@pytest.mark.parametrize("cfg", FAST, ids=[f"n{c[0]}-bs{c[1]}-{c[3]}" for c in FAST])
+def test_register_heat_streams_match_generic_and_oracle(cfg):
+    """Heat with forward Euler takes the register-resident stream kernels;
+    `threads=256` forces the shared-memory streams.  Both, and the standard
+    path, are bitwise the oracle's, frames included."""
+    n, bs, steps, tiling = cfg
+    ic, g = _ic_and_globals("heat", n, steps, True)
+    fast, fast_f = _gpu_frames("heat", ic, g, 1, 1, bs, steps, "swept", **tiling)
+    gen, gen_f = _gpu_frames("heat", ic, g, 1, 1, bs, steps, "swept", threads=256, **tiling)
+    ref, _, _ = oracle.standard("heat", ic, g, 1, steps)
+    assert np.array_equal(fast, ref[: len(fast)])
+    assert np.array_equal(gen, fast)
+    assert np.array_equal(fast_f, gen_f)
