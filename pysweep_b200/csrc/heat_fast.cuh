@@ -87,6 +87,27 @@ __device__ __forceinline__ void heat_pair(double L1u, double L1c, double L1d, do
     n1 = heat_fe(c0, u0, d0, L1c, c1, cr);
 }
 
+// Gap: the four prism face rows of level m at this lane's column pair
+// (upper prism's bottom face rows, then lower prism's top face rows).
+__device__ __forceinline__ void load_faces(const SweptArgs& a, int bup, int band, int HF, int m,
+                                           int cw, int lane, double (&f)[4][2])
+{
+    const int ny = a.ny;
+    const int gm = wrap(cw - m + 2 * lane, ny);
+    const int gm1 = gm + 1 == ny ? 0 : gm + 1;
+    const bool even = (m & 1) == 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int side = q < 2 ? 1 : 0;
+        const int j = q & 1;
+        const int bb = q < 2 ? bup : band;
+        const size_t fo = (((size_t)bb * HF + (m - 1)) * 2 + side) * 2 + j;
+        const double2 v = ld_pair(a.xface + fo * ny, gm, gm1, even);
+        f[q][0] = v.x;
+        f[q][1] = v.y;
+    }
+}
+
 template <int BX, bool GAP>
 __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs a)
 {
@@ -99,7 +120,8 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
     const int H = a.H, Hm = a.Hmax, nx = a.nx, ny = a.ny;
     const int band = unit / a.nseg, seg = unit % a.nseg;
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
-    const int s0 = seg * a.wy;
+    const int s0 = seg_start(a, seg);
+    const int nchunks = (seg_start(a, seg + 1) - s0) / kFastChunk;
     const double cr = a.p.d[0];
     const int CB = Hm * CR * 2;  // one carry buffer: [Hm][CR][2]
     double* carry = sm + (size_t)warp * 2 * CB;
@@ -109,9 +131,9 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
 
     double a0[BX], a1[BX];
     double fb0a = 0.0, fb0b = 0.0, fb1a = 0.0, fb1b = 0.0;  // gap: lower prism's face rows
-    for (int c = 0; c < a.nchunks; ++c) {
+    for (int c = 0; c < nchunks; ++c) {
         const int cw = s0 + c * kFastChunk;
-        const bool first = (c == 0), last = (c == a.nchunks - 1);
+        const bool first = (c == 0), last = (c == nchunks - 1);
         double* cin = carry + (c & 1) * CB;
         double* cout = carry + ((c + 1) & 1) * CB;
         // ---- level 0 ------------------------------------------------------
@@ -154,6 +176,9 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
                 cin[k * 2 + 1] = src[gl1];
             }
         }
+        // gap: the faces of level 1 are read while level 0 settles
+        double nf[4][2];
+        if (GAP && H >= 2) load_faces(a, bup, band, HF, 1, cw, lane, nf);
         __syncwarp();
         for (int m = 1; m <= H; ++m) {
             const double* cr0 = cin + (m - 1) * CR * 2;  // carry of level m-1
@@ -164,7 +189,7 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
             const bool valid = !first || lane >= m;
             int nrow;  // rows of level m held in the arrays
             double lb0a = 0.0, lb0b = 0.0, lb1a = 0.0, lb1b = 0.0;  // prism: last two rows
-            double nf[4][2];  // gap: face rows of level m, prefetched
+            double nn[4][2];  // gap: face rows of level m+1, issued now
             if (!GAP) {
                 // ---- prism: level m rows [m, BX-m) at indices [0, BX-2m) ----
                 // old index i <-> row m-1+i; new index i <-> row m+i
@@ -194,19 +219,9 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
                     lb1b = n1;
                 }
             } else {
-                // ---- gap: prefetch the prisms' face rows of level m ---------
-                if (m <= H - 1) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int side = q < 2 ? 1 : 0;  // 1: upper prism's bottom face
-                        const int j = q & 1;
-                        const int bb = q < 2 ? bup : band;
-                        const size_t fo = (((size_t)bb * HF + (m - 1)) * 2 + side) * 2 + j;
-                        const double2 v = ld_pair(a.xface + fo * ny, gm, gm1, even);
-                        nf[q][0] = v.x;
-                        nf[q][1] = v.y;
-                    }
-                }
+                // ---- gap: issue the prisms' face rows of level m+1 ---------
+                // (level m's rows were issued one level step earlier)
+                if (m + 1 <= H - 1) load_faces(a, bup, band, HF, m + 1, cw, lane, nn);
                 // ---- level m rows [hx-m, hx+m) at indices [2, 2m+2) ----------
                 // old index k <-> row hx-m-1+k for k < 2m; old rows 2m, 2m+1 are
                 // the scalars fb0, fb1; new index k <-> row hx-m-2+k reads old
@@ -247,6 +262,11 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
                     fb0b = nf[2][1];
                     fb1a = nf[3][0];
                     fb1b = nf[3][1];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        nf[q][0] = nn[q][0];
+                        nf[q][1] = nn[q][1];
+                    }
                 }
             }
             // ---- carry of level m for the next chunk (lane 31's columns) ----

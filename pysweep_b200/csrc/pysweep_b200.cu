@@ -14,6 +14,7 @@
 #include "equations.cuh"
 #include "swept.cuh"
 #include "heat_fast.cuh"
+#include "standard_fast.cuh"
 
 namespace psb {
 
@@ -59,6 +60,7 @@ struct ps_solver {
     int mpss = 0;
     // tiling
     int H = 0, nseg = 1, chunk = 32, threads = 128;
+    bool nseg_auto = true;  // choose the segment count per run until configured
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     // named plugin constants
@@ -364,8 +366,7 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     // seam kernels are shared)
     const bool fwd_euler = make_params(s).i[0] != 0;
     if (s->eq == PS_EQ_HEAT && s->its == 1 && fwd_euler && s->threads != 256 &&
-        (s->bs == 16 || s->bs == 32) && s->ny % s->nseg == 0 &&
-        (s->ny / s->nseg) % kFastChunk == 0) {
+        (s->bs == 16 || s->bs == 32) && s->ny % kFastChunk == 0) {
         K.fast = true;
         if (s->bs == 16) {
             K.P = launch_fast<16, false>;
@@ -378,12 +379,28 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     if (s->H < 1 || s->H > s->mpss) return fail(s, PS_ERR_INVALID, "levels per half-cycle %d not in [1, %d]", s->H, s->mpss);
     if (s->chunk < O2 * (s->H + 1))
         return fail(s, PS_ERR_INVALID, "chunk %d narrower than 2*ops*(h+1) = %d", s->chunk, O2 * (s->H + 1));
-    if (s->nseg < 1 || s->ny % s->nseg)
+    if (K.fast) {
+        if (s->nseg < 1 || s->nseg > s->ny / kFastChunk)
+            return fail(s, PS_ERR_INVALID, "nseg %d not in [1, ny/64 = %d]", s->nseg, s->ny / kFastChunk);
+    } else if (s->nseg < 1 || s->ny % s->nseg) {
         return fail(s, PS_ERR_INVALID, "ny %d not divisible into %d segments", s->ny, s->nseg);
+    }
     // the first chunk of a segment shrinks by 2*ops per level on its left edge
-    if (std::min(s->chunk, s->ny / s->nseg) < O2 * (s->H + 1))
+    if (!K.fast && std::min(s->chunk, s->ny / s->nseg) < O2 * (s->H + 1))
         return fail(s, PS_ERR_INVALID, "segment width %d narrower than 2*ops*(h+1) = %d",
                     s->ny / s->nseg, O2 * (s->H + 1));
+    if (s->nseg_auto) {
+        if (K.fast) {
+            // one warp per (band, segment); 3 CTAs of 4 warps per SM fit
+            int sms = 148;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+            const int slots = sms * 3 * kFastWarps;
+            const int nb = s->nx / s->bs;
+            s->nseg = std::max(1, std::min(s->ny / kFastChunk, slots / nb));
+        } else {
+            s->nseg = 1;
+        }
+    }
     const size_t smem = std::max(stream_smem(s), seam_smem(s));
     if (smem > 227 * 1024)
         return fail(s, PS_ERR_UNSUPPORTED, "tile needs %zu bytes of shared memory", smem);
@@ -406,6 +423,8 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     // the last chunk may be partial (generic streams); the register streams
     // use whole 64-column chunks
     a.nchunks = K.fast ? a.wy / kFastChunk : (a.wy + s->chunk - 1) / s->chunk;
+    a.seg_unit = K.fast ? kFastChunk : a.wy;
+    a.seg_units = K.fast ? s->ny / kFastChunk : s->nseg;
     a.its = s->its;
     a.gts_base = gts0 - 1;
     a.xface = s->xface;
@@ -433,13 +452,14 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         double cP = 0, cY = 0, cG = 0, cO = 0;
         for (int m = 1; m <= H; ++m) {
             const double rp = s->bs - 2.0 * s->ops * m, rg = 2.0 * s->ops * m;
-            const double cs = (double)a.wy - 2.0 * s->ops * m, cm = 2.0 * s->ops * m;
+            const double cm = 2.0 * s->ops * m * s->nseg;  // seam columns of a band
+            const double cs = (double)s->ny - cm;           // stream columns of a band
             cP += rp * cs;
             cY += rp * cm;
             cG += rg * cs;
             cO += rg * cm;
         }
-        const double u = (double)units;
+        const double u = (double)a.nb;
         const size_t psm = K.fast ? (s->bs == 16 ? heat_fast_smem<16>(s->H) : heat_fast_smem<32>(s->H))
                                   : stream_smem(s);
         if ((rc = timed_launch(s, 0, cP * u, [&] { K.P(a, units, psm, s->stream); }))) return rc;
@@ -471,6 +491,8 @@ int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_
                                fe * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
     const EqParams prm = make_params(s);
     const int every = frame_every > 0 ? frame_every : 1;
+    // streaming heat kernel (64-column strips); threads = 256 keeps the generic one
+    const bool fast = s->eq == PS_EQ_HEAT && s->ny % 64 == 0 && s->threads != 256;
     int rc;
     for (int64_t L = 1; L <= nlevels; ++L) {
         double* fr = nullptr;
@@ -478,9 +500,20 @@ int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_
             const int64_t slot = (L / its) / every - 1;
             if (slot < frame_cap) fr = frames + (size_t)slot * fe;
         }
+        const int gts = gts0 + (int)(L - 1);
         if ((rc = timed_launch(s, 4, (double)s->nx * s->ny, [&] {
-                 K(s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, s->nv,
-                   gts0 + (int)(L - 1), prm, s->stream);
+                 if (fast) {
+                     const dim3 grid((s->ny / 64 + 7) / 8, (s->nx + kStdRows - 1) / kStdRows);
+                     if (prm.i[0])
+                         heat_standard_fast<false><<<grid, 256, 0, s->stream>>>(
+                             s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, gts, prm.d[0]);
+                     else
+                         heat_standard_fast<true><<<grid, 256, 0, s->stream>>>(
+                             s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, gts, prm.d[0]);
+                 } else {
+                     K(s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, s->nv, gts, prm,
+                       s->stream);
+                 }
              })))
             return rc;
         const int t = p;
@@ -691,7 +724,10 @@ int ps_configure(ps_solver* s, int h, int nseg, int chunk, int threads)
         if (h > s->mpss) return fail(s, PS_ERR_INVALID, "h %d > MPSS %d", h, s->mpss);
         s->H = h;
     }
-    if (nseg) s->nseg = nseg;
+    if (nseg) {
+        s->nseg = nseg;
+        s->nseg_auto = false;
+    }
     if (chunk) {
         if (chunk != 32 && chunk != 64) return fail(s, PS_ERR_INVALID, "chunk must be 32 or 64");
         s->chunk = chunk;

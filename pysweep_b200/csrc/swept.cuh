@@ -57,6 +57,9 @@ struct SweptArgs {
     int Hmax;     // levels the face buffers were sized for
     int nb;       // bands (nx / bx)
     int nseg, wy, nchunks;
+    // column segment s spans [seg_start(s), seg_start(s+1)): boundaries at
+    // multiples of seg_unit, spread as evenly as seg_units allows
+    int seg_unit, seg_units;
     int off;      // first row of prism band 0 (prism bands: off + i*bx)
     int its;
     long long L0;  // global level index of this half-cycle's level 0
@@ -68,6 +71,11 @@ __device__ __forceinline__ int wrap(int v, int n)
 {
     v %= n;
     return v < 0 ? v + n : v;
+}
+
+__device__ __forceinline__ int seg_start(const SweptArgs& a, int s)
+{
+    return a.seg_unit * (int)(((long long)s * a.seg_units) / a.nseg);
 }
 
 // Frame slot for global level L, or -1.
@@ -278,7 +286,7 @@ __global__ void __launch_bounds__(NT) seam_kernel(SweptArgs a)
     double* slot = sm;
     const int unit = blockIdx.x;
     const int band = unit / a.nseg, seg = unit % a.nseg;
-    const int x0 = seg * a.wy;
+    const int x0 = seg_start(a, seg);
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
     const int ul = band * a.nseg + (seg + a.nseg - 1) % a.nseg;  // left stream unit
     const int ur = unit;                                          // right stream unit

@@ -157,6 +157,9 @@ FAST = [
     (256, 16, 29, {"nseg": 4, "h": 5}),
     (128, 32, 20, {"h": 4}),
     (64, 32, 31, {}),
+    (256, 32, 33, {"nseg": 3}),   # uneven segments: 1, 1 and 2 chunks
+    (320, 16, 17, {"nseg": 4}),   # 5 chunks over 4 segments
+    (384, 32, 40, {"nseg": 0}),   # automatic segment count
 ]
 
 
@@ -168,8 +171,26 @@ def test_register_heat_streams_match_generic_and_oracle(cfg):
     n, bs, steps, tiling = cfg
     ic, g = _ic_and_globals("heat", n, steps, True)
     fast, fast_f = _gpu_frames("heat", ic, g, 1, 1, bs, steps, "swept", **tiling)
-    gen, gen_f = _gpu_frames("heat", ic, g, 1, 1, bs, steps, "swept", threads=256, **tiling)
+    # the shared-memory streams need equal segments; any tiling gives the same bits
+    gtiling = {k: v for k, v in tiling.items() if k != "nseg" or (v and n % v == 0)}
+    gen, gen_f = _gpu_frames("heat", ic, g, 1, 1, bs, steps, "swept", threads=256, **gtiling)
     ref, _, _ = oracle.standard("heat", ic, g, 1, steps)
     assert np.array_equal(fast, ref[: len(fast)])
     assert np.array_equal(gen, fast)
     assert np.array_equal(fast_f, gen_f)
+
+
+@pytest.mark.parametrize("scheme,its", [(True, 1), (False, 2)])
+@pytest.mark.parametrize("n", [64, 192, 320])
+def test_streaming_standard_heat_matches_generic_and_oracle(scheme, its, n):
+    """The streaming standard kernel (64-column strips) equals the per-cell
+    generic kernel and the oracle bitwise, frames included."""
+    steps = 23
+    ic, g = _ic_and_globals("heat", n, steps, scheme)
+    nl = steps * its
+    fast, ff = _gpu_frames("heat", ic, g, 1, its, 16, nl, "standard")
+    gen, gf = _gpu_frames("heat", ic, g, 1, its, 16, nl, "standard", threads=256)
+    ref, _, _ = oracle.standard("heat", ic, g, its, nl)
+    assert np.array_equal(fast, gen)
+    assert np.array_equal(ff, gf)
+    assert np.array_equal(fast, ref[: len(fast)])
