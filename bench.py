@@ -184,7 +184,8 @@ def run_reference(args):
 def workload_config(args):
     return {"workload": f"heat2d-fp64-periodic-{args.n}x{args.n}-{args.nsteps}steps-swept",
             "n": args.n, "time_steps": args.nsteps, "blocksize": args.bs,
-            "levels_per_half_cycle": args.h or args.bs // 2 - 1, "nseg": args.nseg,
+            "levels_per_half_cycle": args.h or args.bs // 2 - 1,
+            "nseg": args.nseg or "auto (one wave of warps)",
             "l2": "inputs larger than L2 (field of n*n*8 bytes)"}
 
 
@@ -333,7 +334,7 @@ def main():
     ap.add_argument("--nsteps", type=int, default=5000)
     ap.add_argument("--bs", type=int, default=32)
     ap.add_argument("--h", type=int, default=0)
-    ap.add_argument("--nseg", type=int, default=1)
+    ap.add_argument("--nseg", type=int, default=0, help="column segments per band (0: automatic)")
     ap.add_argument("--standard-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-n", type=int, default=2048)
