@@ -151,6 +151,28 @@ int64_t ps_kernel_launches(const ps_solver *s);
  * of the last failed ps_create on this thread. */
 const char *ps_last_error(const ps_solver *s);
 
+/*
+ * Swept heat solve (forward Euler, the heat plugin's arithmetic) that
+ * allocates nothing.  No counterpart in the reference: it exists for callers
+ * that cannot call cudaMalloc at the time they solve -- code running inside
+ * someone else's CUDA graph capture, a process whose memory pool owns the
+ * device, a real-time loop that must not touch the allocator.  The caller
+ * passes the input and output fields (device pointers, nx*ny doubles, distinct);
+ * every temporary lives in one static device array of 128 MiB that each GPU
+ * holds from library load to process exit.  Sizes whose scratch (one field plus
+ * the prism faces, about 22*nx*ny bytes at blocksize 32) exceeds it are
+ * rejected with PS_ERR_INVALID and a message in err.  The first call on a
+ * device resolves the array's device address, so make it before any stream
+ * capture.  Calls share the array: two calls that overlap on the GPU (other
+ * streams, other host threads) race and corrupt each other.  No part of the
+ * array needs to start at zero (every half-cycle writes what it reads).
+ * Computes nsteps steps of courant = alpha*dt/dx/dx on `stream` (NULL = the
+ * default stream); blocksize 16 or 32, nx a multiple of it, ny of 64.
+ */
+int ps_heat_swept_noalloc(const double *d_in, double *d_out, int nx, int ny, int blocksize,
+                          int64_t nsteps, double alpha, double dt, double dx, void *stream,
+                          char *err, size_t errlen);
+
 /* Library version string. */
 const char *ps_version(void);
 

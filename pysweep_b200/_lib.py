@@ -61,6 +61,10 @@ _SIGS = {
                                        ctypes.POINTER(ctypes.c_double)]),
     "ps_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "ps_version": (ctypes.c_char_p, []),
+    "ps_heat_swept_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
 }
 
 

@@ -1,0 +1,71 @@
+"""ps_heat_swept_noalloc, the entry point for callers that cannot allocate.
+
+Callers inside another framework's graph capture or under a foreign memory
+pool cannot cudaMalloc when they solve; this entry point keeps its scratch in a
+static device array instead.  It must give exactly what the allocating path
+(ps_run on a ps_solver) gives, on consecutive calls that share the array.
+This file is collected last on purpose.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(lib, d_in, d_out, n, bs, steps, g):
+    err = ctypes.create_string_buffer(256)
+    rc = lib.ps_heat_swept_noalloc(ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(d_out.data_ptr()),
+                                   n, n, bs, steps, g[5], g[2], g[3], None, err, 256)
+    return rc, err.value.decode()
+
+
+def _allocating(ic, bs, steps, g):
+    from pysweep_b200 import Engine, plugin_constants
+    with Engine("heat", ic.shape[1], ic.shape[2], its=1, blocksize=bs) as e:
+        for k, v in plugin_constants("heat", g).items():
+            e.set_global(k, v)
+        e.set_state(ic)
+        e.run(steps, mode="swept")
+        return e.get_state()
+
+
+@pytest.mark.parametrize("bs", [16, 32])
+def test_noalloc_matches_allocating_path_on_consecutive_calls(bs):
+    import torch
+    from pysweep_b200 import _lib
+    lib = _lib.lib()
+    n = 512
+    dx = 1.0 / n
+    dt = 0.2 * dx * dx
+    rng = np.random.default_rng(bs)
+    results = []
+    for call, steps in enumerate((47, 33)):  # two calls in a row share the scratch array
+        g = [0.0, steps * dt, dt, dx, dx, 1.0, True]
+        ic = rng.standard_normal((1, n, n))
+        d_in = torch.from_numpy(ic).cuda()
+        d_out = torch.full_like(d_in, float("nan"))
+        rc, msg = _noalloc(lib, d_in, d_out, n, bs, steps, g)
+        assert rc == 0, msg
+        torch.cuda.synchronize()
+        got = d_out.cpu().numpy()
+        ref = _allocating(ic, bs, steps, g)
+        assert np.array_equal(got, ref), f"call {call}: differs by {np.abs(got - ref).max()}"
+        assert np.array_equal(d_in.cpu().numpy(), ic), "input modified"
+        results.append(got)
+    assert not np.array_equal(results[0], results[1])
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    import torch
+    from pysweep_b200 import _lib
+    lib = _lib.lib()
+    n = 4096  # ~370 MB of scratch at blocksize 32
+    d_in = torch.zeros((1, 64, 64), dtype=torch.float64, device="cuda")  # never read
+    d_out = torch.zeros_like(d_in)
+    err = ctypes.create_string_buffer(256)
+    rc = lib.ps_heat_swept_noalloc(ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(d_out.data_ptr()),
+                                   n, n, 32, 10, 1.0, 1e-8, 1.0 / n, None, err, 256)
+    assert rc == -1
+    assert b"scratch" in err.value
