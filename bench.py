@@ -324,6 +324,194 @@ def run_b200(args):
     return 0
 
 
+def batched_instances(seed=1, n_heat=256, n_euler=64):
+    """Sizes (multiples of 32 in [128, 2048]), heat diffusivities U(0.5, 2) and
+    vortex strengths U(1, 5), seeded."""
+    rng = np.random.default_rng(seed)
+    choices = np.arange(128, 2049, 32)
+    heat = [(int(rng.choice(choices)), float(rng.uniform(0.5, 2.0))) for _ in range(n_heat)]
+    euler = [(int(rng.choice(choices)), float(rng.uniform(1.0, 5.0))) for _ in range(n_euler)]
+    return heat, euler
+
+
+def run_batched(args):
+    """Batched persistent launches (one CUDA graph) vs one solver per instance."""
+    import torch
+
+    from pysweep_b200 import Engine, plugin_constants
+    from pysweep_b200.batch import Batch
+    from pysweep_b200.equations.euler import analytical_array
+
+    heat, euler = batched_instances(n_heat=args.batch_heat, n_euler=args.batch_euler)
+    out = {"metric": "batched speedup (per-instance time / batched time)", "unit": "x",
+           "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+           "steps": args.steps, "warmup": args.warmup, "time_steps": args.batched_steps}
+    groups = []
+    for eqn, inst in (("heat", heat), ("euler", euler)):
+        if not inst:
+            continue
+        its = 1 if eqn == "heat" else 2
+        bs = 32 if eqn == "heat" else 16
+        nl = args.batched_steps * its
+        fields, consts = [], []
+        for n, par in inst:
+            if eqn == "heat":
+                dx = 1.0 / n
+                dt = 0.2 * dx * dx / par
+                g = [0.0, 1.0, dt, dx, dx, par, True]
+                fields.append(fourier_field(n, seed=n)[0][None])
+            else:
+                dx = 10.0 / n
+                g = [0.0, 1.0, 0.1 * dx, dx, dx, 1.4]
+                fields.append(analytical_array(n, n, 0.0, strength=par))
+            consts.append(plugin_constants(eqn, g))
+        dev = [torch.from_numpy(np.ascontiguousarray(f)).cuda() for f in fields]
+        cells = float(sum(n * n for n, _ in inst)) * nl
+        # batched
+        b = Batch(eqn, [(n, n) for n, _ in inst], its=its, blocksize=bs)
+        for i in range(len(inst)):
+            b.set_constants(i, consts[i])
+        for _ in range(args.warmup):
+            for i in range(len(inst)):
+                b.set_state(i, dev[i])
+            b.run(nl, graph=True)
+        b.synchronize()
+        t = []
+        for _ in range(args.steps):
+            for i in range(len(inst)):
+                b.set_state(i, dev[i])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.run(nl, graph=True)
+            b.synchronize()
+            t.append(time.perf_counter() - t0)
+        t_batch = statistics.median(t)
+        batch_out = [b.get_state(i) for i in range(min(3, len(inst)))]
+        b.close()
+        # one solver per instance: all on one stream, then each on its own
+        engines = []
+        for i, (n, _) in enumerate(inst):
+            e = Engine(eqn, n, n, its=its, blocksize=bs)
+            for k, v in consts[i].items():
+                e.set_global(k, v)
+            engines.append(e)
+        res = {}
+        shared = torch.cuda.Stream()
+        for label in ("one_stream", "own_streams"):
+            if label == "one_stream":
+                for e in engines:
+                    e.set_stream(shared.cuda_stream)
+            else:
+                for e in engines:
+                    e.set_stream(0)  # back to a stream of its own
+            for _ in range(max(1, args.warmup - 2)):
+                for i, e in enumerate(engines):
+                    e.set_state(dev[i])
+                    e.run(nl)
+                torch.cuda.synchronize()
+            t = []
+            for _ in range(args.steps):
+                for i, e in enumerate(engines):
+                    e.set_state(dev[i])
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for e in engines:
+                    e.run(nl)
+                torch.cuda.synchronize()
+                t.append(time.perf_counter() - t0)
+            res[label] = statistics.median(t)
+        for i in range(len(batch_out)):
+            if not np.array_equal(engines[i].get_state(), batch_out[i]):
+                raise AssertionError(f"batched {eqn} instance {i} differs from its single run")
+        for e in engines:
+            e.close()
+        best = min(res.values())
+        groups.append({"equation": eqn, "instances": len(inst), "time_steps": args.batched_steps,
+                       "blocksize": bs, "batched_s": t_batch, "per_instance_one_stream_s": res["one_stream"],
+                       "per_instance_own_streams_s": res["own_streams"],
+                       "speedup_vs_best_per_instance": best / t_batch,
+                       "batched_gcell_updates_s": cells / t_batch / 1e9})
+    out["groups"] = groups
+    out["value"] = (sum(g["per_instance_one_stream_s"] for g in groups) /
+                    sum(g["batched_s"] for g in groups))
+    out["value_vs_own_streams"] = (sum(g["per_instance_own_streams_s"] for g in groups) /
+                                   sum(g["batched_s"] for g in groups))
+    out["timing"] = "wall clock around the run with device synchronisation on both sides"
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_adjoint(args):
+    """Inverse heat problem: forward vs adjoint cost, gradients vs central differences."""
+    import torch
+
+    from pysweep_b200.adjoint import heat_solve
+
+    n, steps, every = args.adj_n, args.adj_steps, 64
+    rng = np.random.default_rng(2)
+    x = np.arange(n) / n
+
+    def fourier(modes=8):
+        f = np.zeros((n, n))
+        for _ in range(modes):
+            k, l = rng.integers(1, 9, 2)
+            f += rng.uniform(0, 1) * np.sin(2 * np.pi * (k * x[:, None] + l * x[None, :]) +
+                                            rng.uniform(0, 2 * np.pi))
+        return f / modes
+
+    dev = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")  # noqa: E731
+    alpha_star = dev(1.0 + 0.5 * fourier())
+    alpha0 = dev(1.0 + 0.5 * fourier())
+    u0 = dev(fourier())
+    dx = 1.0 / n
+    dt = 0.2 * dx * dx / 1.5  # stable for alpha <= 1.5
+    target = heat_solve(u0, alpha_star, steps, dt, dx, every)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    for _ in range(args.warmup):
+        heat_solve(u0, alpha0, steps, dt, dx, every)
+    fwd, bwd = [], []
+    for _ in range(args.steps):
+        xu = u0.clone().requires_grad_(True)
+        xa = alpha0.clone().requires_grad_(True)
+        t_f, uT = timed(lambda: heat_solve(xu, xa, steps, dt, dx, every))
+        loss = 0.5 * ((uT - target) ** 2).sum()
+        t_b, _ = timed(lambda: loss.backward())
+        fwd.append(t_f)
+        bwd.append(t_b)
+    gu, ga = xu.grad, xa.grad
+
+    def J(a, b):
+        return 0.5 * ((heat_solve(a, b, steps, dt, dx, every) - target) ** 2).sum().item()
+
+    h = 1e-6
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    worst = 0.0
+    for _ in range(args.adj_dirs):
+        du = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=gen)
+        da = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=gen)
+        du /= du.norm()
+        da /= da.norm()
+        fd = (J(u0 + h * du, alpha0 + h * da) - J(u0 - h * du, alpha0 - h * da)) / (2 * h)
+        an = (gu * du).sum().item() + (ga * da).sum().item()
+        worst = max(worst, abs(fd - an) / max(abs(an), 1e-300))
+    t_f, t_b = statistics.median(fwd), statistics.median(bwd)
+    print(json.dumps({
+        "metric": "adjoint/forward cost", "value": t_b / t_f, "unit": "x", "higher_is_better": False,
+        "forward_ms": t_f, "backward_ms": t_b, "n": n, "time_steps": steps, "checkpoint_every": every,
+        "fd_directions": args.adj_dirs, "fd_h": h, "fd_max_rel_err": worst, "dtype": "f64",
+        "data": "synthetic", "steps": args.steps, "warmup": args.warmup}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -340,11 +528,25 @@ def main():
     ap.add_argument("--ref-n", type=int, default=2048)
     ap.add_argument("--ref-cycles", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched", action="store_true",
+                    help="batched instances vs one solver per instance (separate JSON line)")
+    ap.add_argument("--batched-steps", type=int, default=1000)
+    ap.add_argument("--batch-heat", type=int, default=256)
+    ap.add_argument("--batch-euler", type=int, default=64)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="inverse heat problem: adjoint vs forward cost (separate JSON line)")
+    ap.add_argument("--adj-n", type=int, default=2048)
+    ap.add_argument("--adj-steps", type=int, default=2000)
+    ap.add_argument("--adj-dirs", type=int, default=32)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.batched:
+        return run_batched(args)
+    if args.adjoint:
+        return run_adjoint(args)
     return run_b200(args)
 
 

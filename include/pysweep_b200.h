@@ -173,6 +173,58 @@ int ps_heat_swept_noalloc(const double *d_in, double *d_out, int nx, int ny, int
                           int64_t nsteps, double alpha, double dt, double dx, void *stream,
                           char *err, size_t errlen);
 
+/*
+ * Batches: many independent fields (uneven sizes, one equation, one blocksize)
+ * advanced together.  No counterpart in the reference, which runs one field
+ * per Solver; the per-instance equivalent is one ps_solver per field.  Every
+ * phase of a half-cycle is one launch for all instances (a flat table of
+ * (instance, band segment) units); with use_graph != 0 the launches of a whole
+ * run are captured once into a CUDA graph and replayed.  Constants are per
+ * instance (index) or for all (index = -1).  Register streams (heat, forward
+ * Euler, blocksize 16/32) need nx, ny multiples of 32; the other equations use
+ * the shared-memory streams with one segment per band.
+ */
+typedef struct ps_batch ps_batch;
+int ps_batch_create(ps_batch **out, int device, int equation, int count, const int *nx,
+                    const int *ny, int nv, int ops, int its, int blocksize);
+int ps_batch_destroy(ps_batch *b);
+int ps_batch_set_global(ps_batch *b, int index, const char *name, const void *value,
+                        size_t nbytes);
+int ps_batch_set_state(ps_batch *b, int index, const double *src, int levels, int src_on_device);
+int ps_batch_run(ps_batch *b, int64_t nlevels, int use_graph);
+int ps_batch_get_state(ps_batch *b, int index, double *dst, int level, int dst_on_device);
+int ps_batch_synchronize(ps_batch *b);
+int64_t ps_batch_launches(const ps_batch *b);
+int ps_batch_units(const ps_batch *b);
+const char *ps_batch_last_error(const ps_batch *b);
+
+/*
+ * Heat equation with a spatially varying diffusivity alpha(x, y) and its
+ * adjoint.  No counterpart in the reference (its heat plugin has one scalar
+ * ALPHA, pysweep/equations/heat.cu:8); the per-cell update keeps the plugin's
+ * operation order with courant = alpha*dt/dx/dx per cell.  All pointers are
+ * device pointers of nx*ny doubles; ny must be a multiple of 64.
+ *
+ * ps_heatvar_forward: u_T after nsteps steps from u0.  Writes the courant
+ * field to d_courant, uses d_work as scratch, and (if d_checkpoints != NULL)
+ * stores u every `every` steps: checkpoint k = u_{k*every}, k = 0 ..
+ * ceil(nsteps/every)-1.
+ *
+ * ps_heatvar_adjoint: for J(u_T) with d_lamT = dJ/du_T, writes dJ/du0 to
+ * d_lam0 and dJ/dalpha to d_galpha, walking the checkpoint segments backward:
+ * each segment's states are recomputed into d_states (every fields), then the
+ * adjoint steps lambda_n = lambda_{n+1} + L(C .* lambda_{n+1}),
+ * dJ/dC += lambda_{n+1} .* L u_n run backward through it.  d_lamwork is a
+ * scratch field.  `err` receives a message on failure.
+ */
+int ps_heatvar_forward(const double *d_u0, const double *d_alpha, double *d_uT, int nx, int ny,
+                       int64_t nsteps, double dt, double dx, double *d_courant, double *d_work,
+                       double *d_checkpoints, int every, void *stream, char *err, size_t errlen);
+int ps_heatvar_adjoint(const double *d_courant, const double *d_checkpoints, int every,
+                       const double *d_lamT, double *d_lam0, double *d_galpha, int nx, int ny,
+                       int64_t nsteps, double dt, double dx, double *d_states, double *d_lamwork,
+                       void *stream, char *err, size_t errlen);
+
 /* Library version string. */
 const char *ps_version(void);
 

@@ -61,6 +61,33 @@ _SIGS = {
                                        ctypes.POINTER(ctypes.c_double)]),
     "ps_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "ps_version": (ctypes.c_char_p, []),
+    "ps_heatvar_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "ps_heatvar_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
+                                          ctypes.c_size_t]),
+    "ps_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int]),
+    "ps_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "ps_batch_set_global": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p,
+                                           ctypes.c_void_p, ctypes.c_size_t]),
+    "ps_batch_set_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_int, ctypes.c_int]),
+    "ps_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int]),
+    "ps_batch_get_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_int, ctypes.c_int]),
+    "ps_batch_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "ps_batch_launches": (ctypes.c_int64, [ctypes.c_void_p]),
+    "ps_batch_units": (ctypes.c_int, [ctypes.c_void_p]),
+    "ps_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "ps_heat_swept_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_int, ctypes.c_int64,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -87,8 +114,9 @@ def lib():
     return _lib
 
 
-def check(rc, handle=None):
+def check(rc, handle=None, batch=False):
     if rc != PS_OK:
-        msg = lib().ps_last_error(handle)
+        f = lib().ps_batch_last_error if batch else lib().ps_last_error
+        msg = f(handle)
         raise PySweepError(rc, msg.decode() if msg else "")
     return rc

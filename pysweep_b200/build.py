@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpysweep_b200.so")
-SOURCES = ["pysweep_b200.cu", "noalloc.cu"]
+SOURCES = ["pysweep_b200.cu", "noalloc.cu", "adjoint.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
          "-shared"]

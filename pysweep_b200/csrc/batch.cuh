@@ -1,0 +1,64 @@
+// Batched swept phases: many independent instances (uneven grid sizes) advance
+// together, one launch per phase for all of them.
+//
+// Every instance has two descriptors (SweptArgs for even and odd
+// half-cycles: base buffers swapped, prism bands offset by 0 or bs/2) and
+// contributes its (band, segment) units to one flat unit table of
+// (instance, unit) pairs.  A batched launch maps warp / CTA g to table entry g
+// and runs the same body as the single-instance kernel.  All instances share
+// the blocksize, so they share the levels per half-cycle and the shared-memory
+// layout.  The launches of a whole run are captured into one CUDA graph.
+#pragma once
+#include "heat_fast.cuh"
+#include "swept.cuh"
+
+namespace psb {
+
+__device__ __forceinline__ void batch_args(const SweptArgs* __restrict__ desc, int inst,
+                                           int parity, int H, long long L0, SweptArgs& a)
+{
+    a = desc[2 * inst + parity];
+    a.H = H;
+    a.L0 = L0;
+}
+
+template <int BX, bool GAP>
+__global__ void __launch_bounds__(32 * kFastWarps, 3)
+    heat_stream_fast_batch(const SweptArgs* __restrict__ desc, const int2* __restrict__ units,
+                           int nunits, int parity, int H, long long L0)
+{
+    extern __shared__ double sm[];
+    const int warp = threadIdx.x >> 5;
+    const int g = blockIdx.x * kFastWarps + warp;
+    if (g >= nunits) return;  // whole warp
+    const int2 u = units[g];
+    SweptArgs a;
+    batch_args(desc, u.x, parity, H, L0, a);
+    heat_fast_body<BX, GAP>(a, u.y, sm + (size_t)warp * 2 * (a.Hmax * (BX + 2) * 2));
+}
+
+template <class Eq, int ITS, int W, bool GAP, int NT>
+__global__ void __launch_bounds__(NT)
+    stream_batch(const SweptArgs* __restrict__ desc, const int2* __restrict__ units, int parity,
+                 int H, long long L0)
+{
+    extern __shared__ double sm[];
+    const int2 u = units[blockIdx.x];
+    SweptArgs a;
+    batch_args(desc, u.x, parity, H, L0, a);
+    stream_body<Eq, ITS, W, GAP, NT>(a, u.y, sm);
+}
+
+template <class Eq, int ITS, bool GAP, int NT>
+__global__ void __launch_bounds__(NT)
+    seam_batch(const SweptArgs* __restrict__ desc, const int2* __restrict__ units, int parity,
+               int H, long long L0)
+{
+    extern __shared__ double sm[];
+    const int2 u = units[blockIdx.x];
+    SweptArgs a;
+    batch_args(desc, u.x, parity, H, L0, a);
+    seam_body<Eq, ITS, GAP, NT>(a, u.y, sm);
+}
+
+}  // namespace psb

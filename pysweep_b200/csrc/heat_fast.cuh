@@ -108,23 +108,25 @@ __device__ __forceinline__ void load_faces(const SweptArgs& a, int bup, int band
     }
 }
 
+// One (band, segment) unit of one warp; `carry` is the warp's own shared
+// memory (two buffers of [Hmax][BX+2][2]).
 template <int BX, bool GAP>
-__global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs a)
+__device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int unit, double* carry)
 {
-    extern __shared__ double sm[];
     constexpr int hx = BX / 2;
     constexpr int CR = BX + 2;  // carry rows
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int unit = blockIdx.x * kFastWarps + warp;
-    if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
+    const int lane = threadIdx.x & 31;
     const int H = a.H, Hm = a.Hmax, nx = a.nx, ny = a.ny;
     const int band = unit / a.nseg, seg = unit % a.nseg;
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
     const int s0 = seg_start(a, seg);
-    const int nchunks = (seg_start(a, seg + 1) - s0) / kFastChunk;
+    // segments are whole multiples of 32 columns: 64-column chunks, the last
+    // one possibly 32 wide (lanes 16..31 then hold columns past the segment)
+    const int wseg = seg_start(a, seg + 1) - s0;
+    const int nchunks = (wseg + kFastChunk - 1) / kFastChunk;
+    const int lastw = wseg - (nchunks - 1) * kFastChunk;
     const double cr = a.p.d[0];
     const int CB = Hm * CR * 2;  // one carry buffer: [Hm][CR][2]
-    double* carry = sm + (size_t)warp * 2 * CB;
     const int HF = Hm - 1;
     const int bup = wrap(band - 1, a.nb);
     const int r0w = wrap(r0, nx);
@@ -134,6 +136,7 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
     for (int c = 0; c < nchunks; ++c) {
         const int cw = s0 + c * kFastChunk;
         const bool first = (c == 0), last = (c == nchunks - 1);
+        const int nact = last ? lastw / 2 : 32;  // lanes holding this chunk's columns
         double* cin = carry + (c & 1) * CB;
         double* cout = carry + ((c + 1) & 1) * CB;
         // ---- level 0 ------------------------------------------------------
@@ -185,8 +188,9 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
             const int gm = wrap(cw - m + 2 * lane, ny);  // this lane's first column at level m
             const int gm1 = gm + 1 == ny ? 0 : gm + 1;   // and its second
             const bool even = (m & 1) == 0;              // parity of gm (cw and ny are even)
-            // left-seam mask: the first chunk's level m starts at column s0+m (lane m)
-            const bool valid = !first || lane >= m;
+            // left-seam mask: the first chunk's level m starts at column s0+m
+            // (lane m); a 32-column last chunk ends at lane 15
+            const bool valid = (!first || lane >= m) && lane < nact;
             int nrow;  // rows of level m held in the arrays
             double lb0a = 0.0, lb0b = 0.0, lb1a = 0.0, lb1b = 0.0;  // prism: last two rows
             double nn[4][2];  // gap: face rows of level m+1, issued now
@@ -314,7 +318,7 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
 #pragma unroll
                 for (int side = 0; side < 2; ++side) {
                     if ((side == 0 && !first) || (side == 1 && !last)) continue;
-                    const int owner = side == 0 ? m : 31;
+                    const int owner = side == 0 ? m : nact - 1;
                     double* yf = a.yface + (((size_t)unit * 2 + side) * HF + (m - 1)) * BX * 2;
 #pragma unroll
                     for (int i = 0; i < BX; ++i) {
@@ -329,6 +333,16 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
         }
         __syncwarp();
     }
+}
+
+template <int BX, bool GAP>
+__global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs a)
+{
+    extern __shared__ double sm[];
+    const int warp = threadIdx.x >> 5;
+    const int unit = blockIdx.x * kFastWarps + warp;
+    if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
+    heat_fast_body<BX, GAP>(a, unit, sm + (size_t)warp * 2 * (a.Hmax * (BX + 2) * 2));
 }
 
 }  // namespace psb

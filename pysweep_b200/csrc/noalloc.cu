@@ -136,8 +136,8 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
     a.nseg = nseg;
     a.wy = ny / nseg;
     a.nchunks = a.wy / kFastChunk;
-    a.seg_unit = kFastChunk;
-    a.seg_units = ny / kFastChunk;
+    a.seg_unit = 32;
+    a.seg_units = ny / 32;
     a.its = 1;
     a.gts_base = 0;
     a.frame_every = 1;

@@ -15,6 +15,7 @@
 #include "swept.cuh"
 #include "heat_fast.cuh"
 #include "standard_fast.cuh"
+#include "batch.cuh"
 
 namespace psb {
 
@@ -144,15 +145,15 @@ int eq_ops(int eq, int ops)
 
 // Equation constants, computed on the host the way each plugin's set_globals
 // computes its CPU globals (heat.py:37, euler.py:23-24).
-EqParams make_params(const ps_solver* s)
+EqParams make_params_g(int eq, const std::map<std::string, double>& globals)
 {
     EqParams p;
     memset(&p, 0, sizeof p);
     auto g = [&](const char* k, double d) {
-        auto it = s->globals.find(k);
-        return it == s->globals.end() ? d : it->second;
+        auto it = globals.find(k);
+        return it == globals.end() ? d : it->second;
     };
-    switch (s->eq) {
+    switch (eq) {
     case PS_EQ_HEAT: {
         const double alpha = g("ALPHA", 1.0), dt = g("DT", 0.0), dx = g("DX", 1.0);
         p.d[0] = alpha * dt / dx / dx;
@@ -174,6 +175,8 @@ EqParams make_params(const ps_solver* s)
     }
     return p;
 }
+
+EqParams make_params(const ps_solver* s) { return make_params_g(s->eq, s->globals); }
 
 // ------------------------------------------------------------ dispatch ----
 using SweptLaunch = void (*)(const SweptArgs&, int grid, size_t smem, cudaStream_t);
@@ -366,7 +369,7 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     // seam kernels are shared)
     const bool fwd_euler = make_params(s).i[0] != 0;
     if (s->eq == PS_EQ_HEAT && s->its == 1 && fwd_euler && s->threads != 256 &&
-        (s->bs == 16 || s->bs == 32) && s->ny % kFastChunk == 0) {
+        (s->bs == 16 || s->bs == 32) && s->ny % 32 == 0) {
         K.fast = true;
         if (s->bs == 16) {
             K.P = launch_fast<16, false>;
@@ -380,8 +383,8 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     if (s->chunk < O2 * (s->H + 1))
         return fail(s, PS_ERR_INVALID, "chunk %d narrower than 2*ops*(h+1) = %d", s->chunk, O2 * (s->H + 1));
     if (K.fast) {
-        if (s->nseg < 1 || s->nseg > s->ny / kFastChunk)
-            return fail(s, PS_ERR_INVALID, "nseg %d not in [1, ny/64 = %d]", s->nseg, s->ny / kFastChunk);
+        if (s->nseg < 1 || s->nseg > s->ny / 32)
+            return fail(s, PS_ERR_INVALID, "nseg %d not in [1, ny/32 = %d]", s->nseg, s->ny / 32);
     } else if (s->nseg < 1 || s->ny % s->nseg) {
         return fail(s, PS_ERR_INVALID, "ny %d not divisible into %d segments", s->ny, s->nseg);
     }
@@ -397,6 +400,7 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
             const int slots = sms * 3 * kFastWarps;
             const int nb = s->nx / s->bs;
             s->nseg = std::max(1, std::min(s->ny / kFastChunk, slots / nb));
+            s->nseg = std::max(1, std::min(s->nseg, s->ny / 32));
         } else {
             s->nseg = 1;
         }
@@ -423,8 +427,8 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     // the last chunk may be partial (generic streams); the register streams
     // use whole 64-column chunks
     a.nchunks = K.fast ? a.wy / kFastChunk : (a.wy + s->chunk - 1) / s->chunk;
-    a.seg_unit = K.fast ? kFastChunk : a.wy;
-    a.seg_units = K.fast ? s->ny / kFastChunk : s->nseg;
+    a.seg_unit = K.fast ? 32 : a.wy;
+    a.seg_units = K.fast ? s->ny / 32 : s->nseg;
     a.its = s->its;
     a.gts_base = gts0 - 1;
     a.xface = s->xface;
@@ -851,5 +855,437 @@ int ps_set_stream(ps_solver* s, void* stream)
     }
     return PS_OK;
 }
+
+}  // extern "C"
+
+// ====================================================================== batch
+// Many independent instances in one set of launches (include/pysweep_b200.h,
+// ps_batch_*).
+
+struct BatchInst {
+    int nx = 0, ny = 0, nb = 0, nseg = 1;
+    double* base[2] = {nullptr, nullptr};
+    double* xface = nullptr;
+    double* yface = nullptr;
+    bool have_state = false;
+    std::map<std::string, double> globals;
+};
+
+struct ps_batch {
+    int device = 0, eq = 0, nv = 1, ops = 1, its = 1, bs = 0, mpss = 0, H = 0;
+    bool fast = false;
+    cudaStream_t stream = nullptr;
+    std::vector<BatchInst> inst;
+    SweptArgs* d_desc = nullptr;  // [2 * count]: even / odd half-cycles
+    int2* d_units = nullptr;      // (instance, unit) of every band segment
+    int nunits = 0;
+    int cur = 0;                  // base holding the current levels (all instances)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int64_t graph_levels = -1;
+    int graph_cur = -1;
+    int64_t graph_launches = 0;
+    int64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+int bfail(ps_batch* b, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (b) b->err = buf;
+    else g_create_error = buf;
+    return code;
+}
+
+#define PSB_CUDA(b, call)                                                                       \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return bfail((b), e_ == cudaErrorMemoryAllocation ? PS_ERR_NOMEM : PS_ERR_CUDA,     \
+                         "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+bool global_allowed(int eq, const char* name)
+{
+    for (const auto& g : kGlobals)
+        if (!strcmp(g.name, name) && (g.eqmask >> eq & 1)) return true;
+    return false;
+}
+
+void batch_free_graph(ps_batch* b)
+{
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->gexec = nullptr;
+    b->graph = nullptr;
+    b->graph_levels = -1;
+}
+
+// Upload both descriptors of every instance (constants may have changed).
+int batch_upload(ps_batch* b)
+{
+    const int n = (int)b->inst.size();
+    std::vector<SweptArgs> d(2 * n);
+    const int O2 = 2 * b->ops;
+    for (int i = 0; i < n; ++i) {
+        const BatchInst& I = b->inst[i];
+        for (int par = 0; par < 2; ++par) {
+            SweptArgs& a = d[2 * i + par];
+            memset(&a, 0, sizeof a);
+            a.bin = I.base[par];
+            a.bout = I.base[1 - par];
+            a.xface = I.xface;
+            a.yface = I.yface;
+            a.frame_every = 1;
+            a.nx = I.nx;
+            a.ny = I.ny;
+            a.nv = b->nv;
+            a.bx = b->bs;
+            a.hx = b->bs / 2;
+            a.Hmax = b->H;
+            a.nb = I.nb;
+            a.nseg = I.nseg;
+            a.wy = I.ny / I.nseg;
+            a.nchunks = b->fast ? a.wy / kFastChunk : (a.wy + 31) / 32;
+            a.seg_unit = b->fast ? 32 : a.wy;
+            a.seg_units = b->fast ? I.ny / 32 : I.nseg;
+            a.off = par ? b->bs / 2 : 0;  // prism bands alternate by half a block
+            a.its = b->its;
+            a.gts_base = 0;
+            a.p = make_params_g(b->eq, I.globals);
+        }
+        (void)O2;
+    }
+    PSB_CUDA(b, cudaMemcpyAsync(b->d_desc, d.data(), d.size() * sizeof(SweptArgs),
+                                cudaMemcpyHostToDevice, b->stream));
+    PSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    return PS_OK;
+}
+
+size_t batch_stream_smem(const ps_batch* b)
+{
+    if (b->fast) return b->bs == 16 ? heat_fast_smem<16>(b->H) : heat_fast_smem<32>(b->H);
+    const int O2 = 2 * b->ops, RS = 32 + O2;
+    return sizeof(double) * ((size_t)(b->its + 1) * b->nv * b->bs * RS +
+                             (size_t)(b->H + 1) * b->nv * b->bs * O2);
+}
+
+size_t batch_seam_smem(const ps_batch* b)
+{
+    return sizeof(double) * (size_t)(b->its + 1) * b->nv * b->bs * (2 * b->ops * (b->H + 1));
+}
+
+using BatchFast = void (*)(const SweptArgs*, const int2*, int, int, int, long long);
+using BatchGen = void (*)(const SweptArgs*, const int2*, int, int, long long);
+
+struct BatchKernels {
+    const void* P = nullptr;
+    const void* G = nullptr;
+    const void* Y = nullptr;
+    const void* O = nullptr;
+};
+
+// Enqueue one half-cycle for every instance.
+template <class Eq, int ITS>
+void batch_half(ps_batch* b, int par, int H, long long L0, size_t ssm, size_t gsm, dim3 fgrid)
+{
+    const int nu = b->nunits;
+    if (b->fast) {
+        if (b->bs == 16) {
+            heat_stream_fast_batch<16, false><<<fgrid, 32 * kFastWarps, gsm, b->stream>>>(b->d_desc, b->d_units, nu, par, H, L0);
+            seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+            heat_stream_fast_batch<16, true><<<fgrid, 32 * kFastWarps, gsm, b->stream>>>(b->d_desc, b->d_units, nu, par, H, L0);
+            seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+        } else {
+            heat_stream_fast_batch<32, false><<<fgrid, 32 * kFastWarps, gsm, b->stream>>>(b->d_desc, b->d_units, nu, par, H, L0);
+            seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+            heat_stream_fast_batch<32, true><<<fgrid, 32 * kFastWarps, gsm, b->stream>>>(b->d_desc, b->d_units, nu, par, H, L0);
+            seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+        }
+    } else {
+        stream_batch<Eq, ITS, 32, false, 256><<<nu, 256, gsm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+        seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+        stream_batch<Eq, ITS, 32, true, 256><<<nu, 256, gsm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+        seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+    }
+}
+
+template <class Eq, int ITS>
+void batch_prepare()
+{
+    allow_big_smem(heat_stream_fast_batch<16, false>);
+    allow_big_smem(heat_stream_fast_batch<16, true>);
+    allow_big_smem(heat_stream_fast_batch<32, false>);
+    allow_big_smem(heat_stream_fast_batch<32, true>);
+    allow_big_smem(stream_batch<Eq, ITS, 32, false, 256>);
+    allow_big_smem(stream_batch<Eq, ITS, 32, true, 256>);
+    allow_big_smem(seam_batch<Eq, ITS, false, 128>);
+    allow_big_smem(seam_batch<Eq, ITS, true, 128>);
+}
+
+using HalfFn = void (*)(ps_batch*, int, int, long long, size_t, size_t, dim3);
+using PrepFn = void (*)();
+
+bool batch_pick(int eq, int ops, int its, HalfFn* half, PrepFn* prep)
+{
+#define PS_BSET(EQ, OP, IT, T)                          \
+    if (eq == EQ && ops == OP && its == IT) {           \
+        *half = batch_half<T, IT>;                      \
+        *prep = batch_prepare<T, IT>;                   \
+        return true;                                    \
+    }
+    PS_BSET(PS_EQ_HEAT, 1, 1, Heat)
+    PS_BSET(PS_EQ_HEAT, 1, 2, Heat)
+    PS_BSET(PS_EQ_EULER, 2, 2, Euler)
+    PS_BSET(PS_EQ_HALF, 1, 2, Half)
+#undef PS_BSET
+    return false;
+}
+
+// Enqueue a whole run of nlevels levels, starting from parity b->cur.
+int batch_enqueue(ps_batch* b, int64_t nlevels, HalfFn half, int64_t* nlaunch)
+{
+    const size_t ssm = batch_seam_smem(b), gsm = batch_stream_smem(b);
+    const dim3 fgrid((b->nunits + kFastWarps - 1) / kFastWarps);
+    const size_t fe = (size_t)b->nv;
+    int par = b->cur;
+    int64_t done = 0, n = 0;
+    while (done < nlevels) {
+        const int H = (int)std::min<int64_t>(b->H, nlevels - done);
+        if (H < b->its) {  // the newest its-H base levels carry over unchanged
+            for (auto& I : b->inst) {
+                const size_t f = fe * I.nx * I.ny;
+                for (int q = 0; q < b->its - H; ++q)
+                    PSB_CUDA(b, cudaMemcpyAsync(I.base[1 - par] + (size_t)q * f,
+                                                I.base[par] + (size_t)(q + H) * f, f * sizeof(double),
+                                                cudaMemcpyDeviceToDevice, b->stream));
+            }
+        }
+        half(b, par, H, done, ssm, gsm, fgrid);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return bfail(b, PS_ERR_CUDA, "batched launch: %s", cudaGetErrorString(e));
+        n += 4;
+        par ^= 1;
+        done += H;
+    }
+    *nlaunch = n;
+    return PS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ps_batch_destroy(ps_batch* b);
+
+int ps_batch_create(ps_batch** out, int device, int equation, int count, const int* nx,
+                    const int* ny, int nv, int ops, int its, int blocksize)
+{
+    if (!out || count <= 0 || !nx || !ny) return bfail(nullptr, PS_ERR_INVALID, "bad arguments");
+    *out = nullptr;
+    HalfFn half;
+    PrepFn prep;
+    if (!batch_pick(equation, ops, its, &half, &prep))
+        return bfail(nullptr, PS_ERR_UNSUPPORTED, "no batched kernels for equation %d ops %d its %d",
+                     equation, ops, its);
+    if (equation == PS_EQ_EULER && nv != 4) return bfail(nullptr, PS_ERR_INVALID, "euler needs nv=4");
+    if ((equation == PS_EQ_HEAT || equation == PS_EQ_HALF) && nv != 1)
+        return bfail(nullptr, PS_ERR_INVALID, "heat/half need nv=1");
+    if (blocksize % (2 * ops) || blocksize / (2 * ops) - 1 < 1)
+        return bfail(nullptr, PS_ERR_INVALID, "blocksize %d invalid for ops %d", blocksize, ops);
+    ps_batch* b = new ps_batch();
+    b->device = device;
+    b->eq = equation;
+    b->nv = nv;
+    b->ops = ops;
+    b->its = its;
+    b->bs = blocksize;
+    b->mpss = blocksize / (2 * ops) - 1;
+    b->H = b->mpss;
+    b->fast = equation == PS_EQ_HEAT && its == 1 && (blocksize == 16 || blocksize == 32);
+    int rc = PS_OK;
+    std::vector<int2> units;
+    for (int i = 0; i < count && rc == PS_OK; ++i) {
+        BatchInst I;
+        I.nx = nx[i];
+        I.ny = ny[i];
+        if (I.nx % blocksize || I.ny % blocksize || (b->fast && I.ny % 32))
+            rc = bfail(b, PS_ERR_INVALID, "instance %d: %dx%d not divisible by blocksize %d%s", i,
+                       I.nx, I.ny, blocksize, b->fast ? " and 32" : "");
+        else if ((size_t)3 * nv * I.nx * I.ny >= (size_t)1 << 31)
+            rc = bfail(b, PS_ERR_UNSUPPORTED, "instance %d too large for 32-bit offsets", i);
+        else if (!b->fast && 32 < 2 * ops * (b->H + 1))
+            rc = bfail(b, PS_ERR_UNSUPPORTED, "blocksize %d too large for the batched streams", blocksize);
+        I.nb = I.nx / blocksize;
+        // register streams: segments of about four 64-column chunks
+        I.nseg = b->fast ? std::max(1, I.ny / (4 * kFastChunk)) : 1;
+        for (int u = 0; u < I.nb * I.nseg; ++u) units.push_back(make_int2(i, u));
+        b->inst.push_back(I);
+    }
+    if (rc == PS_OK) {
+        cudaError_t e = cudaSetDevice(device);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) rc = bfail(b, PS_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+    }
+    const int O2 = 2 * ops, HF = b->H - 1;
+    for (auto& I : b->inst) {
+        if (rc != PS_OK) break;
+        const size_t f = (size_t)nv * I.nx * I.ny;
+        const size_t xn = (size_t)I.nb * HF * 2 * nv * O2 * I.ny;
+        const size_t yn = (size_t)I.nb * I.nseg * 2 * HF * nv * blocksize * O2;
+        cudaError_t e = cudaMalloc(&I.base[0], f * its * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&I.base[1], f * its * sizeof(double));
+        if (e == cudaSuccess && xn) e = cudaMalloc(&I.xface, xn * sizeof(double));
+        if (e == cudaSuccess && yn) e = cudaMalloc(&I.yface, yn * sizeof(double));
+        if (e != cudaSuccess) rc = bfail(b, PS_ERR_NOMEM, "instance buffers: %s", cudaGetErrorString(e));
+    }
+    if (rc == PS_OK) {
+        b->nunits = (int)units.size();
+        cudaError_t e = cudaMalloc(&b->d_desc, 2 * b->inst.size() * sizeof(SweptArgs));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_units, units.size() * sizeof(int2));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->d_units, units.data(), units.size() * sizeof(int2), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) rc = bfail(b, PS_ERR_NOMEM, "batch tables: %s", cudaGetErrorString(e));
+    }
+    if (rc == PS_OK) prep();
+    if (rc != PS_OK) {
+        g_create_error = b->err;
+        ps_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return PS_OK;
+}
+
+int ps_batch_destroy(ps_batch* b)
+{
+    if (!b) return PS_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_free_graph(b);
+    for (auto& I : b->inst) {
+        for (auto& p : I.base)
+            if (p) cudaFree(p);
+        if (I.xface) cudaFree(I.xface);
+        if (I.yface) cudaFree(I.yface);
+    }
+    if (b->d_desc) cudaFree(b->d_desc);
+    if (b->d_units) cudaFree(b->d_units);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return PS_OK;
+}
+
+int ps_batch_set_global(ps_batch* b, int index, const char* name, const void* value, size_t nbytes)
+{
+    if (!b || !name || !value) return PS_ERR_INVALID;
+    if (!global_allowed(b->eq, name)) return bfail(b, PS_ERR_INVALID, "no constant named %s", name);
+    if (nbytes != 1 && nbytes != 2 && nbytes != 4 && nbytes != 8)
+        return bfail(b, PS_ERR_INVALID, "constant %s: unsupported size %zu", name, nbytes);
+    if (index < -1 || index >= (int)b->inst.size()) return bfail(b, PS_ERR_INVALID, "index %d", index);
+    const double v = decode_value(value, nbytes);
+    for (int i = 0; i < (int)b->inst.size(); ++i)
+        if (index == -1 || index == i) b->inst[i].globals[name] = v;
+    batch_free_graph(b);  // constants live in the captured descriptors
+    return PS_OK;
+}
+
+int ps_batch_set_state(ps_batch* b, int index, const double* src, int levels, int src_on_device)
+{
+    if (!b || !src || index < 0 || index >= (int)b->inst.size()) return PS_ERR_INVALID;
+    if (levels != 1 && levels != b->its) return bfail(b, PS_ERR_INVALID, "levels must be 1 or its");
+    PSB_CUDA(b, cudaSetDevice(b->device));
+    BatchInst& I = b->inst[index];
+    const size_t f = (size_t)b->nv * I.nx * I.ny;
+    for (int q = 0; q < b->its; ++q)
+        PSB_CUDA(b, cudaMemcpyAsync(I.base[b->cur] + (size_t)q * f, src + (size_t)(levels == 1 ? 0 : q) * f,
+                                    f * sizeof(double),
+                                    src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    b->stream));
+    if (!src_on_device) PSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    I.have_state = true;
+    return PS_OK;
+}
+
+int ps_batch_run(ps_batch* b, int64_t nlevels, int use_graph)
+{
+    if (!b) return PS_ERR_INVALID;
+    if (nlevels < 0) return bfail(b, PS_ERR_INVALID, "negative level count");
+    for (size_t i = 0; i < b->inst.size(); ++i)
+        if (!b->inst[i].have_state) return bfail(b, PS_ERR_STATE, "instance %zu has no state", i);
+    PSB_CUDA(b, cudaSetDevice(b->device));
+    HalfFn half;
+    PrepFn prep;
+    batch_pick(b->eq, b->ops, b->its, &half, &prep);
+    const int64_t nhalf = (nlevels + b->H - 1) / b->H;
+    if (!use_graph) {
+        int rc = batch_upload(b);
+        if (rc) return rc;
+        int64_t n = 0;
+        rc = batch_enqueue(b, nlevels, half, &n);
+        if (rc) return rc;
+        b->launches += n;
+    } else {
+        if (!b->gexec || b->graph_levels != nlevels || b->graph_cur != b->cur) {
+            batch_free_graph(b);
+            int rc = batch_upload(b);
+            if (rc) return rc;
+            PSB_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            int64_t n = 0;
+            rc = batch_enqueue(b, nlevels, half, &n);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return bfail(b, PS_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+            b->graph = g;
+            PSB_CUDA(b, cudaGraphInstantiate(&b->gexec, g, 0));
+            b->graph_levels = nlevels;
+            b->graph_cur = b->cur;
+            b->graph_launches = n;
+        }
+        PSB_CUDA(b, cudaGraphLaunch(b->gexec, b->stream));
+        b->launches += b->graph_launches;
+    }
+    b->cur ^= (int)(nhalf & 1);
+    return PS_OK;
+}
+
+int ps_batch_get_state(ps_batch* b, int index, double* dst, int level, int dst_on_device)
+{
+    if (!b || !dst || index < 0 || index >= (int)b->inst.size()) return PS_ERR_INVALID;
+    if (level < 0 || level >= b->its) return bfail(b, PS_ERR_INVALID, "level %d", level);
+    PSB_CUDA(b, cudaSetDevice(b->device));
+    BatchInst& I = b->inst[index];
+    const size_t f = (size_t)b->nv * I.nx * I.ny;
+    PSB_CUDA(b, cudaMemcpyAsync(dst, I.base[b->cur] + (size_t)(b->its - 1 - level) * f,
+                                f * sizeof(double),
+                                dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                b->stream));
+    if (!dst_on_device) PSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    return PS_OK;
+}
+
+int ps_batch_synchronize(ps_batch* b)
+{
+    if (!b) return PS_ERR_INVALID;
+    PSB_CUDA(b, cudaSetDevice(b->device));
+    PSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    return PS_OK;
+}
+
+int64_t ps_batch_launches(const ps_batch* b) { return b ? b->launches : 0; }
+
+const char* ps_batch_last_error(const ps_batch* b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+int ps_batch_units(const ps_batch* b) { return b ? b->nunits : 0; }
 
 }  // extern "C"

@@ -92,9 +92,8 @@ __device__ __forceinline__ long long frame_slot(const SweptArgs& a, long long L)
 // One CTA = one (band, segment) block.  GAP = false: prism (UpPyramid);
 // GAP = true: gap (XBridge) centred on the band's upper boundary row.
 template <class Eq, int ITS, int W, bool GAP, int NT>
-__global__ void __launch_bounds__(NT) stream_kernel(SweptArgs a)
+__device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, double* sm)
 {
-    extern __shared__ double sm[];
     constexpr int OPS = Eq::OPS, O2 = 2 * OPS, RS = W + O2, NSLOT = ITS + 1;
     constexpr int RG = NT / W;  // row groups
     const int nv = a.nv, BX = a.bx, H = a.H, hx = a.hx, nx = a.nx, ny = a.ny;
@@ -102,7 +101,6 @@ __global__ void __launch_bounds__(NT) stream_kernel(SweptArgs a)
     const int CS = nv * BX * O2;  // one carry
     double* slot = sm;
     double* carry = sm + NSLOT * SL;
-    const int unit = blockIdx.x;
     const int band = unit / a.nseg, seg = unit % a.nseg;
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
     const int s0 = seg * a.wy;
@@ -270,21 +268,26 @@ __global__ void __launch_bounds__(NT) stream_kernel(SweptArgs a)
     }
 }
 
+template <class Eq, int ITS, int W, bool GAP, int NT>
+__global__ void __launch_bounds__(NT) stream_kernel(SweptArgs a)
+{
+    extern __shared__ double sm[];
+    stream_body<Eq, ITS, W, GAP, NT>(a, blockIdx.x, sm);
+}
+
 // ------------------------------------------------------------------ seam ----
 // One CTA per (band, segment): the column edge at x0 = seg*wy between segment
 // seg-1 (left) and seg (right).  GAP = false: YBridge; GAP = true: the
 // Octahedron's down half.  Tile columns k <-> global x0 - KC + k, KC = OPS*(Hmax+1).
 template <class Eq, int ITS, bool GAP, int NT>
-__global__ void __launch_bounds__(NT) seam_kernel(SweptArgs a)
+__device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, double* sm)
 {
-    extern __shared__ double sm[];
     constexpr int OPS = Eq::OPS, O2 = 2 * OPS, NSLOT = ITS + 1;
     const int nv = a.nv, BX = a.bx, H = a.H, hx = a.hx, nx = a.nx, ny = a.ny;
     const int KC = OPS * (a.Hmax + 1);
     const int TW = 2 * KC;
     const int SL = nv * BX * TW;
     double* slot = sm;
-    const int unit = blockIdx.x;
     const int band = unit / a.nseg, seg = unit % a.nseg;
     const int x0 = seg_start(a, seg);
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
@@ -406,6 +409,13 @@ __global__ void __launch_bounds__(NT) seam_kernel(SweptArgs a)
             }
         }
     }
+}
+
+template <class Eq, int ITS, bool GAP, int NT>
+__global__ void __launch_bounds__(NT) seam_kernel(SweptArgs a)
+{
+    extern __shared__ double sm[];
+    seam_body<Eq, ITS, GAP, NT>(a, blockIdx.x, sm);
 }
 
 }  // namespace psb
