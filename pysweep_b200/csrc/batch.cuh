@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3)
     const int2 u = units[g];
     SweptArgs a;
     batch_args(desc, u.x, parity, H, L0, a);
-    heat_fast_body<BX, GAP>(a, u.y, sm + (size_t)warp * 2 * (a.Hmax * (BX + 2) * 2));
+    heat_fast_body<BX, GAP>(a, u.y, sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
 template <class Eq, int ITS, int W, bool GAP, int NT>

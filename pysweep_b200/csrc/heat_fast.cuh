@@ -22,9 +22,14 @@
 //     it is updated in place in descending order.
 //
 // Per cell: 8 FP64 operations (numpy's operation order, see Heat in
-// equations.cuh) and one 64-bit shuffle; no shared-memory traffic except the
-// carry, which is double-buffered by chunk parity (the previous chunk's carry
-// is read while this chunk's is written).
+// equations.cuh) and one 64-bit shuffle.  Shared memory holds the carry,
+// double-buffered by chunk parity (the previous chunk's carry is read while
+// this chunk's is written) and packed by level (level j keeps the rows it
+// has), and, in the gap, a ring of the prisms' face rows: the face rows of
+// level m are copied with cp.async kFaceDepth levels before they are needed,
+// which hides the latency of the x-face reads.  The x-faces are stored at the
+// chunk's level-0 columns (xface_col in swept.cuh), so every face access is
+// one aligned 16-byte pair per lane.
 #pragma once
 #include "swept.cuh"
 
@@ -68,12 +73,53 @@ __device__ __forceinline__ double from_left(double v, double carry, int lane)
 
 constexpr int kFastWarps = 4;   // warps (units) per CTA
 constexpr int kFastChunk = 64;  // columns per chunk
+constexpr int kFaceDepth = 3;   // gap: levels of face rows in flight ahead of use
+constexpr int kFaceSlots = kFaceDepth + 1;
+
+// Carry rows kept for levels 0 .. m-1 (the carry of level j holds the rows
+// the level has: BX - 2j for the prism, 2j + 4 for the gap), i.e. the offset
+// of level m's carry in the packed buffer.
+template <int BX, bool GAP>
+__host__ __device__ constexpr int carry_rows(int m)
+{
+    return GAP ? m * (m + 3) : m * BX - m * (m - 1);
+}
+
+// Shared memory of one warp, in doubles: two packed carry buffers (chunk
+// parity) and the gap's ring of face rows ([slot][4 rows][32 lanes][2]).
+template <int BX>
+__host__ __device__ constexpr int heat_fast_warp_doubles(int hmax)
+{
+    return 2 * 2 * (carry_rows<BX, false>(hmax) > carry_rows<BX, true>(hmax)
+                        ? carry_rows<BX, false>(hmax)
+                        : carry_rows<BX, true>(hmax)) +
+           kFaceSlots * 4 * 32 * 2;
+}
 
 template <int BX>
 constexpr size_t heat_fast_smem(int hmax)
 {
-    // per warp: two carry buffers of [hmax][BX+2 rows][2 columns]
-    return sizeof(double) * (size_t)kFastWarps * 2 * hmax * (BX + 2) * 2;
+    return sizeof(double) * (size_t)kFastWarps * heat_fast_warp_doubles<BX>(hmax);
+}
+
+// 16-byte global -> shared copies that complete asynchronously (cp.async,
+// one commit group per level; wait_group<N> waits until at most N groups of
+// this thread are still in flight)
+__device__ __forceinline__ void cp_async16(double* smem, const double* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // A new cell pair from this lane's old rows (up u0, centre c0/c1, down d0)
@@ -87,34 +133,81 @@ __device__ __forceinline__ void heat_pair(double L1u, double L1c, double L1d, do
     n1 = heat_fe(c0, u0, d0, L1c, c1, cr);
 }
 
-// Gap: the four prism face rows of level m at this lane's column pair
-// (upper prism's bottom face rows, then lower prism's top face rows).
-__device__ __forceinline__ void load_faces(const SweptArgs& a, int bup, int band, int HF, int m,
-                                           int cw, int lane, double (&f)[4][2])
+// Gap: start the copy of the four prism face rows of level m at this lane's
+// column pair (upper prism's bottom face rows, then lower prism's top face
+// rows) into one ring slot; gcol is the chunk's level-0 column of the lane.
+__device__ __forceinline__ void issue_faces(const SweptArgs& a, int bup, int band, int HF, int m,
+                                            int gcol, int lane, double* slot)
 {
-    const int ny = a.ny;
-    const int gm = wrap(cw - m + 2 * lane, ny);
-    const int gm1 = gm + 1 == ny ? 0 : gm + 1;
-    const bool even = (m & 1) == 0;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int side = q < 2 ? 1 : 0;
         const int j = q & 1;
         const int bb = q < 2 ? bup : band;
         const size_t fo = (((size_t)bb * HF + (m - 1)) * 2 + side) * 2 + j;
-        const double2 v = ld_pair(a.xface + fo * ny, gm, gm1, even);
-        f[q][0] = v.x;
-        f[q][1] = v.y;
+        cp_async16(slot + (q * 32 + lane) * 2, a.xface + fo * a.ny + gcol);
     }
 }
 
+// Gap: the lower prism's two face rows of level m go to register indices
+// 2m+2 and 2m+3.  m is known only at run time, so a switch names each pair
+// with constant indices (register arrays cannot be indexed dynamically).
+#define PSB_LOWER_CASE(M)                                                                  \
+    case M:                                                                                \
+        if constexpr (2 * (M) + 3 < BX) {                                                  \
+            a0[2 * (M) + 2] = f2.x;                                                        \
+            a1[2 * (M) + 2] = f2.y;                                                        \
+            a0[2 * (M) + 3] = f3.x;                                                        \
+            a1[2 * (M) + 3] = f3.y;                                                        \
+        }                                                                                  \
+        break;
+
+template <int BX>
+__device__ __forceinline__ void place_lower(int m, double2 f2, double2 f3, double (&a0)[BX],
+                                            double (&a1)[BX])
+{
+    static_assert(BX <= 32, "cases cover blocksizes up to 32");
+    switch (m) {
+        PSB_LOWER_CASE(1) PSB_LOWER_CASE(2) PSB_LOWER_CASE(3) PSB_LOWER_CASE(4)
+        PSB_LOWER_CASE(5) PSB_LOWER_CASE(6) PSB_LOWER_CASE(7) PSB_LOWER_CASE(8)
+        PSB_LOWER_CASE(9) PSB_LOWER_CASE(10) PSB_LOWER_CASE(11) PSB_LOWER_CASE(12)
+        PSB_LOWER_CASE(13) PSB_LOWER_CASE(14)
+        default: break;
+    }
+}
+#undef PSB_LOWER_CASE
+
+// Prism: the bottom face rows of level m are the last two of its `count`
+// rows, register indices count-2 and count-1.
+#define PSB_BOTTOM_CASE(C)                                                                 \
+    case C:                                                                                \
+        if constexpr ((C) <= BX) {                                                         \
+            *reinterpret_cast<double2*>(r0) = make_double2(a0[(C) - 2], a1[(C) - 2]);      \
+            *reinterpret_cast<double2*>(r1) = make_double2(a0[(C) - 1], a1[(C) - 1]);      \
+        }                                                                                  \
+        break;
+
+template <int BX>
+__device__ __forceinline__ void store_bottom(int count, const double (&a0)[BX],
+                                             const double (&a1)[BX], double* r0, double* r1)
+{
+    static_assert(BX <= 32, "cases cover blocksizes up to 32");
+    switch (count) {
+        PSB_BOTTOM_CASE(2) PSB_BOTTOM_CASE(4) PSB_BOTTOM_CASE(6) PSB_BOTTOM_CASE(8)
+        PSB_BOTTOM_CASE(10) PSB_BOTTOM_CASE(12) PSB_BOTTOM_CASE(14) PSB_BOTTOM_CASE(16)
+        PSB_BOTTOM_CASE(18) PSB_BOTTOM_CASE(20) PSB_BOTTOM_CASE(22) PSB_BOTTOM_CASE(24)
+        PSB_BOTTOM_CASE(26) PSB_BOTTOM_CASE(28) PSB_BOTTOM_CASE(30) PSB_BOTTOM_CASE(32)
+        default: break;
+    }
+}
+#undef PSB_BOTTOM_CASE
+
 // One (band, segment) unit of one warp; `carry` is the warp's own shared
-// memory (two buffers of [Hmax][BX+2][2]).
+// memory (heat_fast_warp_doubles: two packed carry buffers, then the ring).
 template <int BX, bool GAP>
 __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int unit, double* carry)
 {
     constexpr int hx = BX / 2;
-    constexpr int CR = BX + 2;  // carry rows
     const int lane = threadIdx.x & 31;
     const int H = a.H, Hm = a.Hmax, nx = a.nx, ny = a.ny;
     const int band = unit / a.nseg, seg = unit % a.nseg;
@@ -126,19 +219,26 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
     const int nchunks = (wseg + kFastChunk - 1) / kFastChunk;
     const int lastw = wseg - (nchunks - 1) * kFastChunk;
     const double cr = a.p.d[0];
-    const int CB = Hm * CR * 2;  // one carry buffer: [Hm][CR][2]
+    // one packed carry buffer: level j's rows at carry_rows(j), 2 columns each
+    const int CB = 2 * (carry_rows<BX, false>(Hm) > carry_rows<BX, true>(Hm)
+                            ? carry_rows<BX, false>(Hm)
+                            : carry_rows<BX, true>(Hm));
+    double* ring = carry + 2 * CB;  // gap: [kFaceSlots][4][32][2]
     const int HF = Hm - 1;
     const int bup = wrap(band - 1, a.nb);
     const int r0w = wrap(r0, nx);
 
     double a0[BX], a1[BX];
-    double fb0a = 0.0, fb0b = 0.0, fb1a = 0.0, fb1b = 0.0;  // gap: lower prism's face rows
+    // gap: column 1 of the two rows below the computed ones (the lower
+    // prism's top face rows), for the first computed row's left neighbours
+    double fb0b = 0.0, fb1b = 0.0;
     for (int c = 0; c < nchunks; ++c) {
         const int cw = s0 + c * kFastChunk;
         const bool first = (c == 0), last = (c == nchunks - 1);
         const int nact = last ? lastw / 2 : 32;  // lanes holding this chunk's columns
         double* cin = carry + (c & 1) * CB;
         double* cout = carry + ((c + 1) & 1) * CB;
+        const int gcol = wrap(cw + 2 * lane, ny);  // the lane's level-0 column (x-face column)
         // ---- level 0 ------------------------------------------------------
         {
             const double* b = a.bin;  // its = 1: the only base level
@@ -164,9 +264,11 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                 }
                 const double2 v0 = *reinterpret_cast<const double2*>(rowp(hx) + g);
                 const double2 v1 = *reinterpret_cast<const double2*>(rowp(hx + 1) + g);
-                fb0a = v0.x;
+                a0[2] = v0.x;
+                a1[2] = v0.y;
+                a0[3] = v1.x;
+                a1[3] = v1.y;
                 fb0b = v0.y;
-                fb1a = v1.x;
                 fb1b = v1.y;
             }
             // carry of level 0: columns cw-2 and cw-1 of the level's rows
@@ -179,12 +281,18 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                 cin[k * 2 + 1] = src[gl1];
             }
         }
-        // gap: the faces of level 1 are read while level 0 settles
-        double nf[4][2];
-        if (GAP && H >= 2) load_faces(a, bup, band, HF, 1, cw, lane, nf);
+        // gap: the face rows of levels 1 .. kFaceDepth start arriving; one
+        // commit group per level, empty past the last level with faces
+        if (GAP) {
+#pragma unroll
+            for (int d = 1; d <= kFaceDepth; ++d) {
+                if (d <= H - 1) issue_faces(a, bup, band, HF, d, gcol, lane, ring + d * 256);
+                cp_async_commit();
+            }
+        }
         __syncwarp();
         for (int m = 1; m <= H; ++m) {
-            const double* cr0 = cin + (m - 1) * CR * 2;  // carry of level m-1
+            const double* cr0 = cin + carry_rows<BX, GAP>(m - 1) * 2;  // carry of level m-1
             const int gm = wrap(cw - m + 2 * lane, ny);  // this lane's first column at level m
             const int gm1 = gm + 1 == ny ? 0 : gm + 1;   // and its second
             const bool even = (m & 1) == 0;              // parity of gm (cw and ny are even)
@@ -192,8 +300,6 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
             // (lane m); a 32-column last chunk ends at lane 15
             const bool valid = (!first || lane >= m) && lane < nact;
             int nrow;  // rows of level m held in the arrays
-            double lb0a = 0.0, lb0b = 0.0, lb1a = 0.0, lb1b = 0.0;  // prism: last two rows
-            double nn[4][2];  // gap: face rows of level m+1, issued now
             if (!GAP) {
                 // ---- prism: level m rows [m, BX-m) at indices [0, BX-2m) ----
                 // old index i <-> row m-1+i; new index i <-> row m+i
@@ -214,22 +320,17 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                               n1);
                     a0[i] = n0;
                     a1[i] = n1;
+
                     L1u = L1c;
                     L1c = L1d;
                     cc = cd;
-                    lb0a = lb1a;
-                    lb0b = lb1b;
-                    lb1a = n0;
-                    lb1b = n1;
                 }
             } else {
-                // ---- gap: issue the prisms' face rows of level m+1 ---------
-                // (level m's rows were issued one level step earlier)
-                if (m + 1 <= H - 1) load_faces(a, bup, band, HF, m + 1, cw, lane, nn);
                 // ---- level m rows [hx-m, hx+m) at indices [2, 2m+2) ----------
-                // old index k <-> row hx-m-1+k for k < 2m; old rows 2m, 2m+1 are
-                // the scalars fb0, fb1; new index k <-> row hx-m-2+k reads old
-                // rows k-2 (up), k-1 (centre), k (down).
+                // old index k <-> row hx-m-1+k for k < 2m+2 (indices 2m, 2m+1:
+                // the lower prism's face rows, placed there at the end of the
+                // previous level); new index k <-> row hx-m-2+k reads old rows
+                // k-2 (up), k-1 (centre), k (down).
                 const int K0 = 2 * m + 1;
                 nrow = 2 * m + 2;
                 double2 cc = *reinterpret_cast<const double2*>(cr0 + (K0 - 1) * 2);
@@ -239,11 +340,8 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
 #pragma unroll
                 for (int k = BX - 1; k >= 2; --k) {
                     if (k > K0) continue;
-                    const bool top1 = (k == K0), top2 = (k == K0 - 1);
                     const double u0 = a0[k - 2], u1 = a1[k - 2];
-                    const double c0 = top1 ? fb0a : a0[k - 1];
-                    const double c1 = top1 ? fb0b : a1[k - 1];
-                    const double d0 = top1 ? fb1a : (top2 ? fb0a : a0[k]);
+                    const double c0 = a0[k - 1], c1 = a1[k - 1], d0 = a0[k];
                     const double2 cu = *reinterpret_cast<const double2*>(cr0 + (k - 2) * 2);
                     const double L1u = from_left(u1, cu.y, lane);
                     const double L0c = from_left(c0, cc.x, lane);
@@ -251,40 +349,44 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                     heat_pair(L1u, L1c, L1d, L0c, u0, c0, d0, c1, cr, n0, n1);
                     a0[k] = n0;
                     a1[k] = n1;
+
                     L1d = L1c;
                     L1c = L1u;
                     cc = cu;
                 }
-                // the face rows of level m join: upper at indices 0, 1, lower in
-                // the scalars
+                // the face rows of level m join: upper at indices 0, 1, lower at
+                // 2m+2, 2m+3 (the next level's first centre and down rows).
+                // Each lane reads back only the pairs it copied.
                 if (m <= H - 1) {
-                    a0[0] = nf[0][0];
-                    a1[0] = nf[0][1];
-                    a0[1] = nf[1][0];
-                    a1[1] = nf[1][1];
-                    fb0a = nf[2][0];
-                    fb0b = nf[2][1];
-                    fb1a = nf[3][0];
-                    fb1b = nf[3][1];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        nf[q][0] = nn[q][0];
-                        nf[q][1] = nn[q][1];
-                    }
+                    cp_async_wait<kFaceDepth - 1>();  // level m's group has landed
+                    const double* sl = ring + (m % kFaceSlots) * 256 + lane * 2;
+                    const double2 f0 = *reinterpret_cast<const double2*>(sl + 0 * 64);
+                    const double2 f1 = *reinterpret_cast<const double2*>(sl + 1 * 64);
+                    const double2 f2 = *reinterpret_cast<const double2*>(sl + 2 * 64);
+                    const double2 f3 = *reinterpret_cast<const double2*>(sl + 3 * 64);
+                    a0[0] = f0.x;
+                    a1[0] = f0.y;
+                    a0[1] = f1.x;
+                    a1[1] = f1.y;
+                    place_lower<BX>(m, f2, f3, a0, a1);
+                    fb0b = f2.y;
+                    fb1b = f3.y;
+
+                    // refill the slot of level m-1 (read one level ago)
+                    const int mf = m + kFaceDepth;
+                    if (mf <= H - 1)
+                        issue_faces(a, bup, band, HF, mf, gcol, lane, ring + (mf % kFaceSlots) * 256);
+                    cp_async_commit();
                 }
             }
-            // ---- carry of level m for the next chunk (lane 31's columns) ----
             if (m <= H - 1 && !last) {
-                double* co = cout + m * CR * 2;
+                double* co = cout + carry_rows<BX, GAP>(m) * 2;
+                const int ncarry = GAP ? nrow + 2 : nrow;
 #pragma unroll
                 for (int i = 0; i < BX; ++i) {
-                    if (i >= nrow) break;
+                    if (i >= ncarry) break;
                     if (lane == 31)
                         *reinterpret_cast<double2*>(co + i * 2) = make_double2(a0[i], a1[i]);
-                }
-                if (GAP && lane == 31) {
-                    *reinterpret_cast<double2*>(co + nrow * 2) = make_double2(fb0a, fb0b);
-                    *reinterpret_cast<double2*>(co + (nrow + 1) * 2) = make_double2(fb1a, fb1b);
                 }
             }
             // ---- outputs of level m ------------------------------------------
@@ -293,11 +395,13 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
             const int ibeg = GAP ? 2 : 0;
             const int rfirst = GAP ? hx - m - 2 : m;  // band row of index 0
             if (!GAP && m <= H - 1 && valid) {
+                // faces are stored at the chunk's level-0 columns (xface_col)
                 const size_t fb = ((size_t)band * HF + (m - 1)) * 2;
-                st_pair(a.xface + ((fb + 0) * 2 + 0) * ny, gm, gm1, a0[0], a1[0], even);
-                st_pair(a.xface + ((fb + 0) * 2 + 1) * ny, gm, gm1, a0[1], a1[1], even);
-                st_pair(a.xface + ((fb + 1) * 2 + 0) * ny, gm, gm1, lb0a, lb0b, even);
-                st_pair(a.xface + ((fb + 1) * 2 + 1) * ny, gm, gm1, lb1a, lb1b, even);
+                double* xf = a.xface + gcol;
+                *reinterpret_cast<double2*>(xf + ((fb + 0) * 2 + 0) * ny) = make_double2(a0[0], a1[0]);
+                *reinterpret_cast<double2*>(xf + ((fb + 0) * 2 + 1) * ny) = make_double2(a0[1], a1[1]);
+                store_bottom<BX>(BX - 2 * m, a0, a1, xf + ((fb + 1) * 2 + 0) * ny,
+                                 xf + ((fb + 1) * 2 + 1) * ny);
             }
             const long long fs = frame_slot(a, a.L0 + m);
             if (m == H || fs >= 0) {
@@ -342,7 +446,7 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs
     const int warp = threadIdx.x >> 5;
     const int unit = blockIdx.x * kFastWarps + warp;
     if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
-    heat_fast_body<BX, GAP>(a, unit, sm + (size_t)warp * 2 * (a.Hmax * (BX + 2) * 2));
+    heat_fast_body<BX, GAP>(a, unit, sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
 }  // namespace psb

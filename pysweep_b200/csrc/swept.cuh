@@ -73,6 +73,16 @@ __device__ __forceinline__ int wrap(int v, int n)
     return v < 0 ? v + n : v;
 }
 
+// Column of the x-face buffers that holds grid column g at level m: faces are
+// stored shifted by m columns, so that the register streams, whose chunks
+// slide one column left per level, write and read every level's faces at the
+// chunk's level-0 columns (16-byte aligned pairs).  All kernels use it.
+__device__ __forceinline__ int xface_col(int g, int m, int ny)
+{
+    const int c = g + m;
+    return c >= ny ? c - ny : c;
+}
+
 __device__ __forceinline__ int seg_start(const SweptArgs& a, int s)
 {
     return a.seg_unit * (int)(((long long)s * a.seg_units) / a.nseg);
@@ -196,7 +206,7 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
                     const int g = wrap(cw - OPS * m - O2 + k, ny);
                     const size_t fo =
                         ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                    out[(v * BX + i) * RS + k] = a.xface[fo * ny + g];
+                    out[(v * BX + i) * RS + k] = a.xface[fo * ny + xface_col(g, m, ny)];
                 }
             }
             __syncthreads();
@@ -216,7 +226,7 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
                         const int g = wrap(cw - OPS * m - O2 + k, ny);
                         const size_t fo =
                             ((((size_t)band * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                        a.xface[fo * ny + g] = out[(v * BX + i) * RS + k];
+                        a.xface[fo * ny + xface_col(g, m, ny)] = out[(v * BX + i) * RS + k];
                     }
                 }
                 // base levels of the next half-cycle and frames
@@ -369,7 +379,7 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
                     const int bb = rr < O2 ? bup : bdn;
                     const size_t fo =
                         ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                    out[(v * BX + i) * TW + k] = a.xface[fo * ny + wrap(x0 - KC + k, ny)];
+                    out[(v * BX + i) * TW + k] = a.xface[fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny)];
                 }
             }
         }
@@ -388,7 +398,7 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
                     const int i = side == 0 ? OPS * m + j : BX - OPS * m - O2 + j;
                     const size_t fo =
                         ((((size_t)band * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                    a.xface[fo * ny + wrap(x0 - KC + k, ny)] = out[(v * BX + i) * TW + k];
+                    a.xface[fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny)] = out[(v * BX + i) * TW + k];
                 }
             }
             const bool tob = m > H - ITS;
