@@ -1,5 +1,5 @@
 #!/usr/bin/env python
-"""Benchmark: FP64 swept heat on one B200 (and N replicas under torchrun).
+"""Benchmark: FP64 swept heat on one B200 (row slabs over N GPUs under torchrun).
 
 Workload (one "step" = one full solve): the 2-D heat equation u_t = u_xx + u_yy
 on the periodic unit square, 8192 x 8192 FP64 cells, forward Euler with
@@ -18,6 +18,11 @@ Reported on one JSON line (rank 0):
              bandwidth; above 1.0 means temporal reuse
   cpu_baseline  the reference's CPU swept algorithm (C restatement) on the
              host cores, on a bounded sample of the same workload
+
+Under torchrun with N > 1 ranks the grid is N*8192 x 8192, one 8192-row slab
+per GPU (weak scaling), halo strips exchanged with NCCL after every swept
+half-cycle; `value` counts the cell updates of all ranks over the slowest
+rank's time.
 
 `--impl reference` times that CPU algorithm alone as the reference arm.
 """
@@ -324,6 +329,105 @@ def run_b200(args):
     return 0
 
 
+def run_b200_slabs(args):
+    """N > 1 GPUs: one periodic (N*n) x n grid in row slabs of n rows per GPU
+    (weak scaling), each slab with its own seeded Fourier field, solved with
+    the swept kernels inside each GPU's window and the bs/2-row halo strips
+    exchanged with NCCL point-to-point sends after every half-cycle."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from pysweep_b200 import plugin_constants
+    from pysweep_b200.distributed import SlabSolver
+
+    world = int(os.environ["WORLD_SIZE"])
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    n, steps, bs = args.n, args.nsteps, args.bs
+    sol = SlabSolver("heat", n * world, n, its=1, blocksize=bs, h=args.h, nseg=args.nseg,
+                     device=local)
+    for k, v in plugin_constants("heat", heat_globals(n, steps)).items():
+        sol.set_global(k, v)
+    eng = sol.win.eng
+    slab = fourier_field(n, seed=rank)
+    d_slab = torch.from_numpy(slab).cuda()
+    cells_per_step = float(n) * n * steps  # per rank
+
+    def timed(k, fn):
+        dist.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(k):
+            fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        dist.barrier()
+        t = torch.tensor([ev0.elapsed_time(ev1) / k], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def device_pass():
+        sol.set_slab(d_slab)
+        sol.run(steps)
+
+    for _ in range(args.warmup):
+        device_pass()
+    sol.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = eng.launches
+    eng.profile(True)
+    ms_sw = timed(args.steps, device_pass)
+    prof = eng.profile_read()
+    launches = eng.launches - l0
+    clk = clocks.stop()
+    value = cells_per_step * world / (ms_sw / 1000) / 1e9
+
+    h_in = torch.from_numpy(slab).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+
+    def host_pass():
+        sol.set_slab(h_in.cuda(non_blocking=True))
+        sol.run(steps)
+        h_out.copy_(sol.win.get_rows(sol.halo, sol.rows, 0))
+
+    host_pass()
+    ms_e2e = timed(args.e2e_steps, host_pass)
+    e2e = {"value": cells_per_step * world / (ms_e2e / 1000) / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8),
+           "ms_per_step": ms_e2e, "steps": args.e2e_steps}
+    kinds = {k: v for k, v in prof.items() if v[1] > 0}
+    dom = max(kinds, key=lambda k: kinds[k][0])
+    dms, dn, dcells = kinds[dom]
+    achieved = dcells * CELL_BYTES / (dms / 1000) / 1e9
+    peak, peak_src = measured_peak()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "kernel": dom, "launches": dn,
+            "avg_launch_ms": dms / dn, "algorithmic_bytes_per_launch": dcells * CELL_BYTES / dn,
+            "peak_source": peak_src,
+            "kernel_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()}}
+    cfg = workload_config(args)
+    cfg.update({"workload": f"heat2d-fp64-periodic-{n * world}x{n}-{steps}steps-swept-slabs",
+                "global_rows": n * world, "rows_per_gpu": n, "halo_rows": bs // 2,
+                "parallelism": f"row slabs x{world}, NCCL halo exchange per half-cycle"})
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_sw,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": cfg, "standard": None, "swept_vs_standard": None,
+            "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sol.close()
+    dist.destroy_process_group()
+    return 0
+
+
 def batched_instances(seed=1, n_heat=256, n_euler=64):
     """Sizes (multiples of 32 in [128, 2048]), heat diffusivities U(0.5, 2) and
     vortex strengths U(1, 5), seeded."""
@@ -476,8 +580,10 @@ def run_adjoint(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), r
 
-    for _ in range(args.warmup):
-        heat_solve(u0, alpha0, steps, dt, dx, every)
+    for _ in range(args.warmup):  # both passes, so the timed ones reuse cached buffers
+        xu = u0.clone().requires_grad_(True)
+        xa = alpha0.clone().requires_grad_(True)
+        (0.5 * ((heat_solve(xu, xa, steps, dt, dx, every) - target) ** 2).sum()).backward()
     fwd, bwd = [], []
     for _ in range(args.steps):
         xu = u0.clone().requires_grad_(True)
@@ -492,7 +598,8 @@ def run_adjoint(args):
     def J(a, b):
         return 0.5 * ((heat_solve(a, b, steps, dt, dx, every) - target) ** 2).sum().item()
 
-    h = 1e-6
+    # Richardson-extrapolated central differences: (4 D(h/2) - D(h)) / 3
+    h = 1e-3
     gen = torch.Generator(device="cuda").manual_seed(0)
     worst = 0.0
     for _ in range(args.adj_dirs):
@@ -500,14 +607,15 @@ def run_adjoint(args):
         da = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=gen)
         du /= du.norm()
         da /= da.norm()
-        fd = (J(u0 + h * du, alpha0 + h * da) - J(u0 - h * du, alpha0 - h * da)) / (2 * h)
+        d = lambda e: (J(u0 + e * du, alpha0 + e * da) - J(u0 - e * du, alpha0 - e * da)) / (2 * e)  # noqa: E731
+        fd = (4 * d(h / 2) - d(h)) / 3
         an = (gu * du).sum().item() + (ga * da).sum().item()
         worst = max(worst, abs(fd - an) / max(abs(an), 1e-300))
     t_f, t_b = statistics.median(fwd), statistics.median(bwd)
     print(json.dumps({
         "metric": "adjoint/forward cost", "value": t_b / t_f, "unit": "x", "higher_is_better": False,
         "forward_ms": t_f, "backward_ms": t_b, "n": n, "time_steps": steps, "checkpoint_every": every,
-        "fd_directions": args.adj_dirs, "fd_h": h, "fd_max_rel_err": worst, "dtype": "f64",
+        "fd_directions": args.adj_dirs, "fd_h": h, "fd": "richardson central", "fd_max_rel_err": worst, "dtype": "f64",
         "data": "synthetic", "steps": args.steps, "warmup": args.warmup}), flush=True)
     return 0
 
@@ -547,6 +655,8 @@ def main():
         return run_batched(args)
     if args.adjoint:
         return run_adjoint(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        return run_b200_slabs(args)
     return run_b200(args)
 
 

@@ -125,6 +125,17 @@ int ps_run(ps_solver *s, int mode, int64_t nlevels, int gts0, double *frames, in
  * Replaces the memcpy_dtoh after each phase group (functions.py:32). */
 int ps_get_state(ps_solver *s, double *dst, int level, int dst_on_device);
 
+/* Copy rows [row0, row0+nrows) of every variable of base level `level`
+ * (0 = newest) to / from a packed [nv][nrows][ny] buffer.  These move the
+ * edge strips of a row slab between ranks after each swept half-cycle:
+ * they replace the numpy copy of the last/first `splitx` rows that
+ * sendForward / sendBackward hand to MPI Sendrecv and write back into the
+ * shared array (pysweep/core/functions.py:101-123, rows split among ranks in
+ * pysweep/core/process.py:131-176).  Host buffers make the call blocking. */
+int ps_get_rows(ps_solver *s, int level, int row0, int nrows, double *dst, int dst_on_device);
+int ps_set_rows(ps_solver *s, int level, int row0, int nrows, const double *src,
+                int src_on_device);
+
 /* Wait for all work queued on the solver's stream; returns the first device
  * error seen (PS_ERR_TIMEOUT when a bounded wait gave up). */
 int ps_synchronize(ps_solver *s);

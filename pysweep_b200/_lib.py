@@ -51,6 +51,10 @@ _SIGS = {
     "ps_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
                               ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
     "ps_get_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "ps_get_rows": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_void_p, ctypes.c_int]),
+    "ps_set_rows": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_void_p, ctypes.c_int]),
     "ps_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "ps_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "ps_kernel_launches": (ctypes.c_int64, [ctypes.c_void_p]),

@@ -11,12 +11,18 @@
 // The forward stores u every `every` steps; the backward pass walks the
 // segments from the last to the first, recomputes the segment's states from
 // its checkpoint into a work buffer, then runs the adjoint steps backward
-// through the segment; each adjoint step updates lambda and accumulates the
-// gradient in one pass.
+// through the segment.
 //
-// All kernels stream 64-column strips down 32-row blocks: lane l holds columns
-// 2l, 2l+1, the rows above/at/below in registers, lateral neighbours by
-// shuffle (the layout of heat_standard_fast).
+// All kernels stream 64-column strips down blocks of rows: lane l holds
+// columns 2l, 2l+1, the rows above/at/below in registers, lateral neighbours
+// by shuffle (the layout of heat_standard_fast).  The backward pass fuses two
+// time steps per launch, both in the recompute (u_n -> u_{n+1}, u_{n+2}) and
+// in the adjoint (lambda_{n+1} -> lambda_{n-1}, gradient of both steps added
+// with one read and one write of dJ/dC): the first step is also evaluated on
+// one halo row above and below the strip and one halo column either side, so
+// the second step finds its neighbours in registers.  Every cell sees the
+// same operations in the same order as in the one-step kernels, so fused and
+// unfused passes agree bitwise.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,23 +35,26 @@
 namespace psb {
 namespace {
 
-constexpr int kRows = 32;
-
 struct Strip {
-    int nx, ny, g, x0, xend, lane, hcol;
-    __device__ Strip(int nx_, int ny_) : nx(nx_), ny(ny_)
+    int nx, ny, g, x0, xend, lane, hcol, hcol2;
+    __device__ Strip(int nx_, int ny_, int rows) : nx(nx_), ny(ny_)
     {
         const int warp = threadIdx.x >> 5;
         lane = threadIdx.x & 31;
         const int cw = (blockIdx.x * 8 + warp) * 64;
         g = cw + 2 * lane;
-        x0 = blockIdx.y * kRows;
-        xend = min(x0 + kRows, nx);
+        x0 = blockIdx.y * rows;
+        xend = min(x0 + rows, nx);
+        // halo columns: lane 0 holds cw-1 and cw-2, lane 31 cw+64 and cw+65 (periodic)
         const int gl = cw == 0 ? ny - 1 : cw - 1;
+        const int gl2 = gl == 0 ? ny - 1 : gl - 1;
         const int gr = cw + 64 == ny ? 0 : cw + 64;
+        const int gr2 = gr + 1 == ny ? 0 : gr + 1;
         hcol = lane == 0 ? gl : gr;
+        hcol2 = lane == 0 ? gl2 : gr2;
     }
     __device__ bool active() const { return g - 2 * lane < ny; }
+    __device__ bool edge() const { return lane == 0 || lane == 31; }
     __device__ size_t row(int x) const
     {
         x += x < 0 ? nx : 0;
@@ -59,6 +68,12 @@ struct Row {
     double a, b, h;
 };
 
+// a row with the second halo column too (h2: cw-2 on lane 0, cw+65 on lane 31)
+struct Row2 {
+    double a, b, h, h2;
+    __device__ Row row() const { return Row{a, b, h}; }
+};
+
 __device__ __forceinline__ Row load_row(const double* f, const Strip& s, int x)
 {
     const double* p = f + s.row(x);
@@ -66,8 +81,31 @@ __device__ __forceinline__ Row load_row(const double* f, const Strip& s, int x)
     Row r;
     r.a = v.x;
     r.b = v.y;
-    r.h = (s.lane == 0 || s.lane == 31) ? p[s.hcol] : 0.0;
+    r.h = s.edge() ? p[s.hcol] : 0.0;
     return r;
+}
+
+__device__ __forceinline__ Row2 load_row2(const double* f, const Strip& s, int x)
+{
+    const double* p = f + s.row(x);
+    const double2 v = *reinterpret_cast<const double2*>(p + s.g);
+    Row2 r;
+    r.a = v.x;
+    r.b = v.y;
+    r.h = s.edge() ? p[s.hcol] : 0.0;
+    r.h2 = s.edge() ? p[s.hcol2] : 0.0;
+    return r;
+}
+
+__device__ __forceinline__ Row2 mul_row2(const Row2& c, const Row2& l)
+{
+    return Row2{__dmul_rn(c.a, l.a), __dmul_rn(c.b, l.b), __dmul_rn(c.h, l.h),
+                __dmul_rn(c.h2, l.h2)};
+}
+
+__device__ __forceinline__ void store_pair(double* f, const Strip& s, int x, double v0, double v1)
+{
+    *reinterpret_cast<double2*>(f + s.row(x) + s.g) = make_double2(v0, v1);
 }
 
 // 5-point operator ((f[x+1]-2f)+f[x-1]) + ((f[y+1]-2f)+f[y-1]) for the pair
@@ -84,6 +122,36 @@ __device__ __forceinline__ void lap(const Row& up, const Row& c, const Row& dn, 
                    __dadd_rn(__fma_rn(-2.0, c.b, right), c.a));
 }
 
+// the same operator on the halo column of lanes 0 (cw-1) and 31 (cw+64)
+__device__ __forceinline__ double lap_halo(const Row2& up, const Row2& c, const Row2& dn, int lane)
+{
+    const double left = lane == 0 ? c.h2 : c.b;
+    const double right = lane == 0 ? c.a : c.h2;
+    return __dadd_rn(__dadd_rn(__fma_rn(-2.0, c.h, dn.h), up.h),
+                     __dadd_rn(__fma_rn(-2.0, c.h, right), left));
+}
+
+// one forward step at the pair
+__device__ __forceinline__ void fe_pair(const Row& up, const Row& c, const Row& dn, double ca,
+                                        double cb, int lane, double& n0, double& n1)
+{
+    double left = __shfl_up_sync(0xffffffffu, c.b, 1);
+    double right = __shfl_down_sync(0xffffffffu, c.a, 1);
+    if (lane == 0) left = c.h;
+    if (lane == 31) right = c.h;
+    n0 = heat_fe(c.a, up.a, dn.a, left, c.b, ca);
+    n1 = heat_fe(c.b, up.b, dn.b, c.a, right, cb);
+}
+
+// one forward step on the halo column
+__device__ __forceinline__ double fe_halo(const Row2& up, const Row2& c, const Row2& dn, double ch,
+                                          int lane)
+{
+    const double ym = lane == 0 ? c.h2 : c.b;
+    const double yp = lane == 0 ? c.a : c.h2;
+    return heat_fe(c.h, up.h, dn.h, ym, yp, ch);
+}
+
 __global__ void courant_kernel(const double* __restrict__ alpha, double* __restrict__ C, size_t n,
                                double dt, double dx)
 {
@@ -95,24 +163,55 @@ __global__ void courant_kernel(const double* __restrict__ alpha, double* __restr
 // u' = (C*dxx + C*dyy) + u
 __global__ void __launch_bounds__(256) heatvar_step(const double* __restrict__ u,
                                                     const double* __restrict__ C,
-                                                    double* __restrict__ out, int nx, int ny)
+                                                    double* __restrict__ out, int nx, int ny,
+                                                    int rows)
 {
-    const Strip s(nx, ny);
+    const Strip s(nx, ny, rows);
     if (!s.active()) return;
     Row up = load_row(u, s, s.x0 - 1), ce = load_row(u, s, s.x0);
     for (int x = s.x0; x < s.xend; ++x) {
         const Row dn = load_row(u, s, x + 1);
-        double left = __shfl_up_sync(0xffffffffu, ce.b, 1);
-        double right = __shfl_down_sync(0xffffffffu, ce.a, 1);
-        if (s.lane == 0) left = ce.h;
-        if (s.lane == 31) right = ce.h;
-        const size_t o = s.row(x) + s.g;
-        const double2 cr = *reinterpret_cast<const double2*>(C + o);
-        const double n0 = heat_fe(ce.a, up.a, dn.a, left, ce.b, cr.x);
-        const double n1 = heat_fe(ce.b, up.b, dn.b, ce.a, right, cr.y);
-        *reinterpret_cast<double2*>(out + o) = make_double2(n0, n1);
+        const double2 cr = *reinterpret_cast<const double2*>(C + s.row(x) + s.g);
+        double n0, n1;
+        fe_pair(up, ce, dn, cr.x, cr.y, s.lane, n0, n1);
+        store_pair(out, s, x, n0, n1);
         up = ce;
         ce = dn;
+    }
+}
+
+// Two forward steps: mid = step(u), out = step(mid).  The first step runs on
+// rows x0-1 .. xend and on the halo columns.
+__global__ void __launch_bounds__(256) heatvar_step2(const double* __restrict__ u,
+                                                     const double* __restrict__ C,
+                                                     double* __restrict__ mid,
+                                                     double* __restrict__ out, int nx, int ny,
+                                                     int rows)
+{
+    const Strip s(nx, ny, rows);
+    if (!s.active()) return;
+    Row2 uu = load_row2(u, s, s.x0 - 2), uc = load_row2(u, s, s.x0 - 1);
+    Row cc = load_row(C, s, s.x0 - 1);
+    Row cp{0.0, 0.0, 0.0};  // C one row up (own columns)
+    Row mu{0.0, 0.0, 0.0}, mc{0.0, 0.0, 0.0};  // first-step rows i-2, i-1
+    for (int i = s.x0 - 1; i <= s.xend; ++i) {
+        const Row2 ud = load_row2(u, s, i + 1);
+        const Row cn = i < s.xend ? load_row(C, s, i + 1) : Row{0.0, 0.0, 0.0};
+        Row m;
+        fe_pair(uu.row(), uc.row(), ud.row(), cc.a, cc.b, s.lane, m.a, m.b);
+        m.h = fe_halo(uu, uc, ud, cc.h, s.lane);
+        if (i >= s.x0 && i < s.xend) store_pair(mid, s, i, m.a, m.b);
+        if (i > s.x0) {
+            double o0, o1;
+            fe_pair(mu, mc, m, cp.a, cp.b, s.lane, o0, o1);
+            store_pair(out, s, i - 1, o0, o1);
+        }
+        uu = uc;
+        uc = ud;
+        cp = cc;
+        cc = cn;
+        mu = mc;
+        mc = m;
     }
 }
 
@@ -121,9 +220,10 @@ __global__ void __launch_bounds__(256) heatvar_adjoint(const double* __restrict_
                                                        const double* __restrict__ C,
                                                        const double* __restrict__ u,
                                                        double* __restrict__ lam_out,
-                                                       double* __restrict__ gC, int nx, int ny)
+                                                       double* __restrict__ gC, int nx, int ny,
+                                                       int rows)
 {
-    const Strip s(nx, ny);
+    const Strip s(nx, ny, rows);
     if (!s.active()) return;
     auto mu_row = [&](int x) {
         const Row l = load_row(lam, s, x), c = load_row(C, s, x);
@@ -153,6 +253,70 @@ __global__ void __launch_bounds__(256) heatvar_adjoint(const double* __restrict_
     }
 }
 
+// Two adjoint levels: from lam = lambda_{n+1}, u_hi = u_n and u_lo = u_{n-1},
+//     lambda_n     = lam + L(C .* lam)            (rows x0-1 .. xend, halo columns)
+//     lambda_{n-1} = lambda_n + L(C .* lambda_n)  -> lam_out
+//     gC += lam .* L(u_hi);  gC += lambda_n .* L(u_lo)   (one read, one write)
+// Iteration i evaluates the first level at row i and the second at row i-1.
+__global__ void __launch_bounds__(256) heatvar_adjoint2(
+    const double* __restrict__ lam, const double* __restrict__ C, const double* __restrict__ u_hi,
+    const double* __restrict__ u_lo, double* __restrict__ lam_out, double* __restrict__ gC, int nx,
+    int ny, int rows)
+{
+    const Strip s(nx, ny, rows);
+    if (!s.active()) return;
+    Row2 lc = load_row2(lam, s, s.x0 - 1), cc = load_row2(C, s, s.x0 - 1);
+    Row2 m1u = mul_row2(load_row2(C, s, s.x0 - 2), load_row2(lam, s, s.x0 - 2));
+    Row2 m1c = mul_row2(cc, lc);
+    Row hu = load_row(u_hi, s, s.x0 - 1), hc = load_row(u_hi, s, s.x0);
+    Row lu = load_row(u_lo, s, s.x0 - 1), lcur = load_row(u_lo, s, s.x0);
+    Row m0u{0.0, 0.0, 0.0}, m0c{0.0, 0.0, 0.0};  // C .* lambda_n, rows i-2, i-1
+    double ln0 = 0.0, ln1 = 0.0;                  // lambda_n at row i-1
+    double g0 = 0.0, g1 = 0.0;                    // gC after the first level, row i-1
+    for (int i = s.x0 - 1; i <= s.xend; ++i) {
+        const Row2 ld = load_row2(lam, s, i + 1), cd = load_row2(C, s, i + 1);
+        const Row2 m1d = mul_row2(cd, ld);
+        // first level at row i
+        double a0, a1;
+        lap(m1u.row(), m1c.row(), m1d.row(), s.lane, a0, a1);
+        const double ah = lap_halo(m1u, m1c, m1d, s.lane);
+        const Row ln{__dadd_rn(lc.a, a0), __dadd_rn(lc.b, a1), __dadd_rn(lc.h, ah)};
+        const Row m0{__dmul_rn(cc.a, ln.a), __dmul_rn(cc.b, ln.b), __dmul_rn(cc.h, ln.h)};
+        double ng0 = 0.0, ng1 = 0.0;
+        if (i >= s.x0 && i < s.xend) {
+            const Row hd = load_row(u_hi, s, i + 1);
+            double q0, q1;
+            lap(hu, hc, hd, s.lane, q0, q1);
+            const double2 gold = *reinterpret_cast<const double2*>(gC + s.row(i) + s.g);
+            ng0 = __fma_rn(lc.a, q0, gold.x);
+            ng1 = __fma_rn(lc.b, q1, gold.y);
+            hu = hc;
+            hc = hd;
+        }
+        // second level at row i-1
+        if (i > s.x0) {
+            const Row ldn = load_row(u_lo, s, i);
+            double b0, b1, q0, q1;
+            lap(m0u, m0c, m0, s.lane, b0, b1);
+            lap(lu, lcur, ldn, s.lane, q0, q1);
+            store_pair(lam_out, s, i - 1, __dadd_rn(ln0, b0), __dadd_rn(ln1, b1));
+            store_pair(gC, s, i - 1, __fma_rn(ln0, q0, g0), __fma_rn(ln1, q1, g1));
+            lu = lcur;
+            lcur = ldn;
+        }
+        m1u = m1c;
+        m1c = m1d;
+        lc = ld;
+        cc = cd;
+        m0u = m0c;
+        m0c = m0;
+        ln0 = ln.a;
+        ln1 = ln.b;
+        g0 = ng0;
+        g1 = ng1;
+    }
+}
+
 __global__ void scale_kernel(double* __restrict__ g, size_t n, double f)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -160,7 +324,20 @@ __global__ void scale_kernel(double* __restrict__ g, size_t n, double f)
         g[i] *= f;
 }
 
-dim3 strip_grid(int nx, int ny) { return dim3((ny / 64 + 7) / 8, (nx + kRows - 1) / kRows); }
+// Rows per strip: 32, halved while the grid has fewer than about 24 warps per
+// SM of a 148-SM part (the kernels stream rows one after the other, so small
+// grids need more, shorter strips to keep loads in flight).
+int adj_rows(int nx, int ny)
+{
+    int rows = 32;
+    while (rows > 8 && (long long)(ny / 64) * ((nx + rows - 1) / rows) < 148LL * 24) rows /= 2;
+    return rows;
+}
+
+dim3 strip_grid(int nx, int ny, int rows)
+{
+    return dim3((ny / 64 + 7) / 8, (nx + rows - 1) / rows);
+}
 
 }  // namespace
 }  // namespace psb
@@ -198,6 +375,7 @@ extern "C" int ps_heatvar_forward(const double* d_u0, const double* d_alpha, dou
     }
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)nx * ny;
+    const int rows = adj_rows(nx, ny);
     courant_kernel<<<1024, 256, 0, st>>>(d_alpha, d_courant, n, dt, dx);
     // ping-pong between d_work and d_uT so that the last step lands in d_uT
     const double* in = d_u0;
@@ -210,7 +388,7 @@ extern "C" int ps_heatvar_forward(const double* d_u0, const double* d_alpha, dou
                         err, errlen);
     for (int64_t k = 0; k < nsteps; ++k) {
         double* out = ((nsteps - 1 - k) % 2 == 0) ? d_uT : d_work;
-        heatvar_step<<<strip_grid(nx, ny), 256, 0, st>>>(in, d_courant, out, nx, ny);
+        heatvar_step<<<strip_grid(nx, ny, rows), 256, 0, st>>>(in, d_courant, out, nx, ny, rows);
         if (d_checkpoints && (k + 1) % every == 0 && k + 1 < nsteps)
             if ((rc = adj_cuda(cudaMemcpyAsync(d_checkpoints + (size_t)((k + 1) / every) * n, out,
                                                n * sizeof(double), cudaMemcpyDeviceToDevice, st),
@@ -235,28 +413,50 @@ extern "C" int ps_heatvar_adjoint(const double* d_courant, const double* d_check
     }
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)nx * ny;
-    const dim3 grid = strip_grid(nx, ny);
-    if ((rc = adj_cuda(cudaMemsetAsync(d_galpha, 0, n * sizeof(double), st), err, errlen))) return rc;
-    // lambda ping-pong: d_lam0 and d_lamwork, arranged so that lambda_0 lands in d_lam0
-    if ((rc = adj_cuda(cudaMemcpyAsync(nsteps % 2 == 0 ? d_lam0 : d_lamwork, d_lamT, n * sizeof(double),
-                                       cudaMemcpyDeviceToDevice, st), err, errlen)))
-        return rc;
-    double* lam = nsteps % 2 == 0 ? d_lam0 : d_lamwork;
+    const int rows = adj_rows(nx, ny);
+    const dim3 grid = strip_grid(nx, ny, rows);
     const int64_t nseg = (nsteps + every - 1) / every;
+    // adjoint launches: two levels per launch, one more for an odd segment
+    int64_t launches = 0;
+    for (int64_t sidx = 0; sidx < nseg; ++sidx) {
+        const int64_t len = std::min<int64_t>((sidx + 1) * every, nsteps) - sidx * every;
+        launches += len / 2 + len % 2;
+    }
+    if ((rc = adj_cuda(cudaMemsetAsync(d_galpha, 0, n * sizeof(double), st), err, errlen))) return rc;
+    // lambda ping-pong between d_lam0 and d_lamwork, arranged so that lambda_0
+    // lands in d_lam0
+    double* lam = launches % 2 == 0 ? d_lam0 : d_lamwork;
+    if ((rc = adj_cuda(cudaMemcpyAsync(lam, d_lamT, n * sizeof(double), cudaMemcpyDeviceToDevice, st),
+                       err, errlen)))
+        return rc;
     for (int64_t sidx = nseg - 1; sidx >= 0; --sidx) {
-        const int64_t n0 = sidx * every, n1 = std::min<int64_t>(n0 + every, nsteps);
-        // states u_{n0} .. u_{n1-1} of this segment
+        const int64_t n0 = sidx * every, len = std::min<int64_t>(n0 + every, nsteps) - n0;
+        // states u_{n0} .. u_{n0+len-1} of this segment
         const double* ck = d_checkpoints + (size_t)sidx * n;
         if ((rc = adj_cuda(cudaMemcpyAsync(d_states, ck, n * sizeof(double), cudaMemcpyDeviceToDevice,
                                            st), err, errlen)))
             return rc;
-        for (int64_t j = 1; j < n1 - n0; ++j)
+        int64_t j = 1;
+        for (; j + 1 < len; j += 2)
+            heatvar_step2<<<grid, 256, 0, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
+                                                d_states + (size_t)j * n,
+                                                d_states + (size_t)(j + 1) * n, nx, ny, rows);
+        if (j < len)
             heatvar_step<<<grid, 256, 0, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
-                                               d_states + (size_t)j * n, nx, ny);
-        for (int64_t nn = n1 - 1; nn >= n0; --nn) {
+                                               d_states + (size_t)j * n, nx, ny, rows);
+        // adjoint levels k = len-1 .. 0 of the segment (lambda_{n0+k+1} -> lambda_{n0+k})
+        int64_t k = len - 1;
+        for (; k >= 1; k -= 2) {
             double* out = lam == d_lam0 ? d_lamwork : d_lam0;
-            heatvar_adjoint<<<grid, 256, 0, st>>>(lam, d_courant, d_states + (size_t)(nn - n0) * n, out,
-                                                  d_galpha, nx, ny);
+            heatvar_adjoint2<<<grid, 256, 0, st>>>(lam, d_courant, d_states + (size_t)k * n,
+                                                   d_states + (size_t)(k - 1) * n, out, d_galpha,
+                                                   nx, ny, rows);
+            lam = out;
+        }
+        if (k == 0) {
+            double* out = lam == d_lam0 ? d_lamwork : d_lam0;
+            heatvar_adjoint<<<grid, 256, 0, st>>>(lam, d_courant, d_states, out, d_galpha, nx, ny,
+                                                  rows);
             lam = out;
         }
     }

@@ -806,6 +806,43 @@ int ps_get_state(ps_solver* s, double* dst, int level, int dst_on_device)
     return PS_OK;
 }
 
+// rows [row0, row0+nrows) of every variable of one base level <-> a packed
+// [nv][nrows][ny] buffer: one strided copy (variables are nx*ny apart)
+static int rows_copy(ps_solver* s, int level, int row0, int nrows, double* buf, int on_device,
+                     bool to_buf)
+{
+    if (!s || !buf) return PS_ERR_INVALID;
+    if (level < 0 || level >= s->its) return fail(s, PS_ERR_INVALID, "level %d not in [0, its)", level);
+    if (row0 < 0 || nrows < 0 || row0 + nrows > s->nx)
+        return fail(s, PS_ERR_INVALID, "rows [%d, %d) outside [0, %d)", row0, row0 + nrows, s->nx);
+    if (nrows == 0) return PS_OK;
+    PS_CUDA(s, cudaSetDevice(s->device));
+    const size_t fe = field_elems(s), plane = (size_t)s->nx * s->ny;
+    double* f = s->base[s->cur] + (size_t)(s->its - 1 - level) * fe + (size_t)row0 * s->ny;
+    const size_t width = (size_t)nrows * s->ny * sizeof(double);
+    if (to_buf)
+        PS_CUDA(s, cudaMemcpy2DAsync(buf, width, f, plane * sizeof(double), width, s->nv,
+                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                     s->stream));
+    else
+        PS_CUDA(s, cudaMemcpy2DAsync(f, plane * sizeof(double), buf, width, width, s->nv,
+                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                     s->stream));
+    if (!on_device) PS_CUDA(s, cudaStreamSynchronize(s->stream));
+    return PS_OK;
+}
+
+int ps_get_rows(ps_solver* s, int level, int row0, int nrows, double* dst, int dst_on_device)
+{
+    return rows_copy(s, level, row0, nrows, dst, dst_on_device, true);
+}
+
+int ps_set_rows(ps_solver* s, int level, int row0, int nrows, const double* src, int src_on_device)
+{
+    if (s && !s->have_state) return fail(s, PS_ERR_STATE, "ps_set_rows before ps_set_state");
+    return rows_copy(s, level, row0, nrows, const_cast<double*>(src), src_on_device, false);
+}
+
 int ps_synchronize(ps_solver* s)
 {
     if (!s) return PS_ERR_INVALID;

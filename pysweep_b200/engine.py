@@ -89,6 +89,31 @@ class Engine:
               self._h)
         return a
 
+    def get_rows(self, row0, nrows, level=0, out=None):
+        """Rows [row0, row0+nrows) of base level `level` (0 = newest) as a
+        (nv, nrows, ny) array, or into `out` (numpy or torch CUDA)."""
+        if out is not None and _is_torch_cuda(out):
+            check(_lib.lib().ps_get_rows(self._h, level, row0, nrows,
+                                         ctypes.c_void_p(out.data_ptr()), 1), self._h)
+            return out
+        a = out if out is not None else np.empty((self.nv, nrows, self.ny))
+        check(_lib.lib().ps_get_rows(self._h, level, row0, nrows,
+                                     a.ctypes.data_as(ctypes.c_void_p), 0), self._h)
+        return a
+
+    def set_rows(self, row0, rows, level=0):
+        """Overwrite rows [row0, row0+k) of base level `level` from a
+        (nv, k, ny) array (numpy or torch CUDA)."""
+        if _is_torch_cuda(rows):
+            k = rows.numel() // (self.nv * self.ny)
+            check(_lib.lib().ps_set_rows(self._h, level, row0, k,
+                                         ctypes.c_void_p(rows.data_ptr()), 1), self._h)
+            return
+        a = np.ascontiguousarray(rows, dtype=np.float64)
+        k = a.size // (self.nv * self.ny)
+        check(_lib.lib().ps_set_rows(self._h, level, row0, k, a.ctypes.data_as(ctypes.c_void_p), 0),
+              self._h)
+
     def run(self, nlevels, mode="swept", gts0=1, frames=None, frame_every=1):
         """Advance `nlevels` levels.  frames: None, a host array or a device tensor of
         shape (k, nv, nx, ny) receiving every `frame_every`-th full step."""

@@ -55,16 +55,45 @@ def test_gradients_match_torch_autograd(every):
         assert rel < 1e-11, rel
 
 
+def test_fused_and_single_step_backward_agree_bitwise():
+    """Segments of one step run only the one-step kernels; longer segments run
+    the two-step fused recompute and adjoint kernels (plus one single step for
+    odd lengths).  Both evaluate every cell with the same operations."""
+    from pysweep_b200.adjoint import heat_solve
+    n, steps = 128, 37
+    u0, alpha, target = _fields(n, 4)
+    dx = 1.0 / n
+    dt = 0.2 * dx * dx / 1.5
+    grads = []
+    for every in (1, 64, 9):
+        x = u0.clone().requires_grad_(True)
+        y = alpha.clone().requires_grad_(True)
+        (0.5 * ((heat_solve(x, y, steps, dt, dx, every) - target) ** 2).sum()).backward()
+        grads.append((x.grad, y.grad))
+    for g in grads[1:]:
+        assert bool((g[0] == grads[0][0]).all()) and bool((g[1] == grads[0][1]).all())
+
+
 def test_gradients_match_central_differences():
+    """Directional derivatives against Richardson-extrapolated central
+    differences, (4 D(h/2) - D(h)) / 3 with D(h) = (J(+h) - J(-h)) / 2h, along
+    unit-norm directions.  The truncation error is O(h^4) (J is exactly
+    quadratic in u0, and smooth in alpha); the roundoff of the four J values
+    (J is a few hundred here) is about 1.5 * eps * J / h.  The test allows
+    1e-7 relative plus 20 * eps * J / h."""
     import torch
     from pysweep_b200.adjoint import heat_solve
-    n, steps, h = 256, 200, 1e-6
+    n, steps, h = 256, 200, 1e-2
     u0, alpha, target = _fields(n, 3)
     dx = 1.0 / n
     dt = 0.2 * dx * dx / 1.5
 
     def J(a, b):
         return 0.5 * ((heat_solve(a, b, steps, dt, dx, 64) - target) ** 2).sum().item()
+
+    def richardson(f):
+        d = lambda e: (f(e) - f(-e)) / (2 * e)  # noqa: E731
+        return (4 * d(h / 2) - d(h)) / 3
 
     x = u0.clone().requires_grad_(True)
     y = alpha.clone().requires_grad_(True)
@@ -75,9 +104,10 @@ def test_gradients_match_central_differences():
         da = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=gen)
         du /= du.norm()
         da /= da.norm()
-        fd_u = (J(u0 + h * du, alpha) - J(u0 - h * du, alpha)) / (2 * h)
-        fd_a = (J(u0, alpha + h * da) - J(u0, alpha - h * da)) / (2 * h)
+        fd_u = richardson(lambda e: J(u0 + e * du, alpha))
+        fd_a = richardson(lambda e: J(u0, alpha + e * da))
         an_u = (x.grad * du).sum().item()
         an_a = (y.grad * da).sum().item()
-        assert abs(fd_u - an_u) <= 1e-6 * max(abs(an_u), 1e-3), (fd_u, an_u)
-        assert abs(fd_a - an_a) <= 1e-6 * max(abs(an_a), 1e-3), (fd_a, an_a)
+        round_off = 20 * np.finfo(np.float64).eps * J(u0, alpha) / h
+        assert abs(fd_u - an_u) <= 1e-7 * abs(an_u) + round_off, (fd_u, an_u)
+        assert abs(fd_a - an_a) <= 1e-7 * abs(an_a) + round_off, (fd_a, an_a)
