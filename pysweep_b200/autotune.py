@@ -1,7 +1,7 @@
 """Autotuner for the swept decomposition's tiling.
 
 For a given equation and grid shape it times candidate tilings -- blocksize
-(rows per band, which sets the maximum levels per half-cycle), levels per
+(8, 16, 32, 64: rows per band, which sets the maximum levels per half-cycle), levels per
 half-cycle h, and column segments per band (how many units, i.e. warps or
 CTAs, share the GPU) -- on the real shape with a short run, and keeps the
 fastest.  Every tiling computes bit-identical results (the swept decomposition
@@ -21,8 +21,8 @@ import numpy as np
 
 from .engine import Engine, plugin_constants
 
-DEFAULT_BLOCKSIZES = {"heat": (16, 32, 64), "euler": (16, 32), "half": (16, 32),
-                      "example": (16, 32), "checker": (16, 32)}
+DEFAULT_BLOCKSIZES = {"heat": (8, 16, 32, 64), "euler": (8, 16, 32, 64), "half": (8, 16, 32),
+                      "example": (8, 16, 32), "checker": (8, 16, 32)}
 
 
 def _cache_path():
