@@ -16,16 +16,19 @@
 //   * every register index is a compile-time constant.  The prism
 //     (UpPyramid) keeps level m's rows [m, BX-m) at indices [0, BX-2m): the
 //     shrinking range is a prefix, updated in place in ascending order with an
-//     early exit.  The gap (XBridge) keeps level m's rows [hx-m-2, hx+m)
-//     (two face rows of the upper prism plus its own rows) at indices
-//     [0, 2m+2) and the two face rows of the lower prism in scalar registers;
-//     it is updated in place in descending order.
+//     early exit.  The gap (XBridge) keeps level m-1's rows [hx-m-1, hx+m+1)
+//     (two face rows of the upper prism, its own rows, two face rows of the
+//     lower prism) at indices [0, 2m+2) and updates them in place in
+//     descending order, entering at the level's first row through a switch
+//     (Duff's device).  Each gap row computes its own left neighbours from
+//     the arrays and the carry, so no value travels from one row to the next
+//     and the entry points cost no register moves.
 //
 // Per cell: 8 FP64 operations (numpy's operation order, see Heat in
-// equations.cuh) and one 64-bit shuffle.  Shared memory holds the carry,
-// double-buffered by chunk parity (the previous chunk's carry is read while
-// this chunk's is written) and packed by level (level j keeps the rows it
-// has), and, in the gap, a ring of the prisms' face rows: the face rows of
+// equations.cuh) and one (prism) or two (gap) 64-bit shuffles.  Shared memory
+// holds the carry, double-buffered by chunk parity (the previous chunk's carry
+// is read while this chunk's is written) and packed by level (level j keeps
+// the rows it has), and, in the gap, a ring of the prisms' face rows: the face rows of
 // level m are copied with cp.async kFaceDepth levels before they are needed,
 // which hides the latency of the x-face reads.  The x-faces are stored at the
 // chunk's level-0 columns (xface_col in swept.cuh), so every face access is
@@ -45,7 +48,7 @@ __device__ __forceinline__ double heat_fe(double c, double xm, double xp, double
 
 // A lane's column pair starts on an even column at even levels and on an odd
 // column at odd levels (the chunk shifts one column per level); 16-byte
-// vector accesses are only legal in the even case (`even` is warp-uniform).
+// vector stores are only legal in the even case (`even` is warp-uniform).
 // In the odd case the pair may straddle the periodic column boundary, so the
 // second column index g1 is wrapped separately.
 __device__ __forceinline__ void st_pair(double* row, int g, int g1, double x, double y, bool even)
@@ -56,12 +59,6 @@ __device__ __forceinline__ void st_pair(double* row, int g, int g1, double x, do
         row[g] = x;
         row[g1] = y;
     }
-}
-
-__device__ __forceinline__ double2 ld_pair(const double* row, int g, int g1, bool even)
-{
-    if (even) return *reinterpret_cast<const double2*>(row + g);
-    return make_double2(row[g], row[g1]);
 }
 
 // Left neighbour's value: shfl_up for lanes 1..31, the carry for lane 0.
@@ -109,6 +106,13 @@ __device__ __forceinline__ void cp_async16(double* smem, const double* gmem)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// 8-byte copy (cp.async.ca: the 4- and 8-byte sizes go through L1)
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
 __device__ __forceinline__ void cp_async_commit()
@@ -202,6 +206,28 @@ __device__ __forceinline__ void store_bottom(int count, const double (&a0)[BX],
 }
 #undef PSB_BOTTOM_CASE
 
+// Gap: row K of level m from old rows K-2 (up), K-1 (centre), K (down) and
+// their carried left columns; self-contained, so that no value travels from
+// one row to the next (rows are entered at the level's first row).
+template <int K, int BX>
+__device__ __forceinline__ void gap_row(double (&a0)[BX], double (&a1)[BX], const double* cr0,
+                                        int lane, double cr)
+{
+    if constexpr (K >= 2 && K < BX) {
+        const double2 cu = *reinterpret_cast<const double2*>(cr0 + (K - 2) * 2);
+        const double2 cc = *reinterpret_cast<const double2*>(cr0 + (K - 1) * 2);
+        const double2 cd = *reinterpret_cast<const double2*>(cr0 + K * 2);
+        const double L1u = from_left(a1[K - 2], cu.y, lane);
+        const double L1c = from_left(a1[K - 1], cc.y, lane);
+        const double L1d = from_left(a1[K], cd.y, lane);
+        const double L0c = from_left(a0[K - 1], cc.x, lane);
+        double n0, n1;
+        heat_pair(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], cr, n0, n1);
+        a0[K] = n0;
+        a1[K] = n1;
+    }
+}
+
 // One (band, segment) unit of one warp; `carry` is the warp's own shared
 // memory (heat_fast_warp_doubles: two packed carry buffers, then the ring).
 template <int BX, bool GAP>
@@ -229,9 +255,6 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
     const int r0w = wrap(r0, nx);
 
     double a0[BX], a1[BX];
-    // gap: column 1 of the two rows below the computed ones (the lower
-    // prism's top face rows), for the first computed row's left neighbours
-    double fb0b = 0.0, fb1b = 0.0;
     for (int c = 0; c < nchunks; ++c) {
         const int cw = s0 + c * kFastChunk;
         const bool first = (c == 0), last = (c == nchunks - 1);
@@ -268,8 +291,6 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                 a1[2] = v0.y;
                 a0[3] = v1.x;
                 a1[3] = v1.y;
-                fb0b = v0.y;
-                fb1b = v1.y;
             }
             // carry of level 0: columns cw-2 and cw-1 of the level's rows
             const int nrow0 = GAP ? 4 : BX;
@@ -320,7 +341,6 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                               n1);
                     a0[i] = n0;
                     a1[i] = n1;
-
                     L1u = L1c;
                     L1c = L1d;
                     cc = cd;
@@ -333,26 +353,70 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                 // k-2 (up), k-1 (centre), k (down).
                 const int K0 = 2 * m + 1;
                 nrow = 2 * m + 2;
-                double2 cc = *reinterpret_cast<const double2*>(cr0 + (K0 - 1) * 2);
-                const double2 cdn = *reinterpret_cast<const double2*>(cr0 + K0 * 2);
-                double L1d = from_left(fb1b, cdn.y, lane);
-                double L1c = from_left(fb0b, cc.y, lane);
-#pragma unroll
-                for (int k = BX - 1; k >= 2; --k) {
-                    if (k > K0) continue;
-                    const double u0 = a0[k - 2], u1 = a1[k - 2];
-                    const double c0 = a0[k - 1], c1 = a1[k - 1], d0 = a0[k];
-                    const double2 cu = *reinterpret_cast<const double2*>(cr0 + (k - 2) * 2);
-                    const double L1u = from_left(u1, cu.y, lane);
-                    const double L0c = from_left(c0, cc.x, lane);
-                    double n0, n1;
-                    heat_pair(L1u, L1c, L1d, L0c, u0, c0, d0, c1, cr, n0, n1);
-                    a0[k] = n0;
-                    a1[k] = n1;
-
-                    L1d = L1c;
-                    L1c = L1u;
-                    cc = cu;
+                // rows K0 .. 2, entered at K0 = 2m+1 and falling through
+                switch (K0) {
+                case 31:
+                    gap_row<31, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<30, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 29:
+                    gap_row<29, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<28, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 27:
+                    gap_row<27, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<26, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 25:
+                    gap_row<25, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<24, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 23:
+                    gap_row<23, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<22, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 21:
+                    gap_row<21, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<20, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 19:
+                    gap_row<19, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<18, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 17:
+                    gap_row<17, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<16, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 15:
+                    gap_row<15, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<14, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 13:
+                    gap_row<13, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<12, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 11:
+                    gap_row<11, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<10, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 9:
+                    gap_row<9, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<8, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 7:
+                    gap_row<7, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<6, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 5:
+                    gap_row<5, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<4, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                case 3:
+                    gap_row<3, BX>(a0, a1, cr0, lane, cr);
+                    gap_row<2, BX>(a0, a1, cr0, lane, cr);
+                    [[fallthrough]];
+                default:
+                    break;
                 }
                 // the face rows of level m join: upper at indices 0, 1, lower at
                 // 2m+2, 2m+3 (the next level's first centre and down rows).
@@ -369,8 +433,6 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                     a0[1] = f1.x;
                     a1[1] = f1.y;
                     place_lower<BX>(m, f2, f3, a0, a1);
-                    fb0b = f2.y;
-                    fb1b = f3.y;
 
                     // refill the slot of level m-1 (read one level ago)
                     const int mf = m + kFaceDepth;
