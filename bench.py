@@ -25,6 +25,8 @@ half-cycle; `value` counts the cell updates of all ranks over the slowest
 rank's time.
 
 `--impl reference` times that CPU algorithm alone as the reference arm.
+`--batched`, `--adjoint` and `--euler` print the batched-instances, adjoint
+and Euler lines instead.
 """
 import argparse
 import json
@@ -221,13 +223,18 @@ def run_b200(args):
         return float(t.item())
 
     n, steps, bs = args.n, args.nsteps, args.bs
-    ic = fourier_field(n, seed=0)
+    f32 = args.f32
+    metric = METRIC.replace("FP64", "FP32") if f32 else METRIC
+    cell_bytes = CELL_BYTES // 2 if f32 else CELL_BYTES
+    ic = fourier_field(n, seed=0).astype(np.float32 if f32 else np.float64)
     g = heat_globals(n, steps)
-    eng = Engine("heat", n, n, its=1, blocksize=bs, device=local)
+    eng = Engine("heat", n, n, its=1, blocksize=bs, device=local,
+                 dtype="float32" if f32 else "float64")
     for k, v in plugin_constants("heat", g).items():
         eng.set_global(k, v)
     eng.configure(h=args.h, nseg=args.nseg)
     stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)  # the solver and torch share one stream: no extra waits
     eng.set_stream(stream.cuda_stream)
     d_ic = torch.from_numpy(ic).cuda()
     cells_per_step = float(n) * n * steps
@@ -270,7 +277,7 @@ def run_b200(args):
                "steps": args.standard_steps}
         pk = prof_st["standard"]
         if pk[1]:
-            std["kernel_effective_gbs"] = pk[2] * CELL_BYTES / (pk[0] / 1000) / 1e9
+            std["kernel_effective_gbs"] = pk[2] * cell_bytes / (pk[0] / 1000) / 1e9
 
     # end to end through the public API with pinned host buffers
     h_in = torch.from_numpy(ic).pin_memory()
@@ -298,23 +305,27 @@ def run_b200(args):
     kinds = {k: v for k, v in prof.items() if v[1] > 0}
     dom = max(kinds, key=lambda k: kinds[k][0])
     dms, dn, dcells = kinds[dom]
-    achieved = dcells * CELL_BYTES / (dms / 1000) / 1e9
+    achieved = dcells * cell_bytes / (dms / 1000) / 1e9
     peak, peak_src = measured_peak()
-    traffic = ncu_traffic(dom, n, bs)
+    traffic = None if f32 else ncu_traffic(dom, n, bs)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "kernel": dom,
             "launches": dn, "avg_launch_ms": dms / dn,
-            "algorithmic_bytes_per_launch": dcells * CELL_BYTES / dn,
+            "algorithmic_bytes_per_launch": dcells * cell_bytes / dn,
             "peak_source": peak_src,
             "kernel_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()}}
 
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+    cfg = workload_config(args)
+    if f32:
+        cfg["workload"] = cfg["workload"].replace("fp64", "fp32")
+    line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_sw,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(args), "standard": std,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 storage, f64 arithmetic" if f32 else "f64",
+            "data": "synthetic", "config": cfg, "standard": std,
             "swept_vs_standard": (value / std["value"]) if std else None,
             "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not f32:
         threads = os.cpu_count() or 1
         v, secs = cpu_baseline(args.ref_n, bs, args.ref_cycles, threads)
         line["cpu_baseline"] = {
@@ -425,6 +436,73 @@ def run_b200_slabs(args):
         print(json.dumps(line), flush=True)
     sol.close()
     dist.destroy_process_group()
+    return 0
+
+
+def euler_field(n, seed=0, modes=8, gamma=1.4):
+    """Uniform state (rho = 1, u = v = 1, p = 1) plus 8 seeded periodic Fourier
+    modes on rho and p, scaled so that the perturbation's maximum is 0.1;
+    conserved variables (rho, rho u, rho v, E)."""
+    f = fourier_field(n, seed=seed, modes=modes)[0]
+    f *= 0.1 / np.abs(f).max()
+    rho, p = 1.0 + f, 1.0 + f
+    out = np.empty((4, n, n))
+    out[0] = rho
+    out[1] = rho
+    out[2] = rho
+    out[3] = p / (gamma - 1) + 0.5 * rho * 2.0
+    return out
+
+
+def run_euler(args):
+    """Euler swept vs standard on one GPU (vortex-free periodic field of Fourier
+    modes, CFL 0.1, two RK stages per step); one JSON line."""
+    import torch
+
+    from pysweep_b200 import Engine, plugin_constants
+
+    n, steps, bs = args.euler_n, args.euler_steps, args.euler_bs
+    dx = 10.0 / n
+    g = [0.0, steps * 0.1 * dx, 0.1 * dx, dx, dx, 1.4]
+    d_ic = torch.from_numpy(euler_field(n)).cuda()
+    eng = Engine("euler", n, n, its=2, blocksize=bs)
+    for k, v in plugin_constants("euler", g).items():
+        eng.set_global(k, v)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    eng.set_stream(stream.cuda_stream)
+    nl = 2 * steps
+    cells = float(n) * n * nl
+
+    def timed(mode, k):
+        for _ in range(3):  # warm-up on a short run
+            eng.set_state(d_ic)
+            eng.run(40, mode=mode)
+        eng.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eng.profile(True)
+        ev0.record(stream)
+        for _ in range(k):
+            eng.set_state(d_ic)
+            eng.run(nl, mode=mode)
+        ev1.record(stream)
+        eng.synchronize()
+        return ev0.elapsed_time(ev1) / k, eng.profile_read()
+
+    ms_sw, prof = timed("swept", args.steps)
+    out_sw = eng.get_state()
+    ms_st, _ = timed("standard", args.steps)
+    out_st = eng.get_state()
+    kinds = {k: v[0] for k, v in prof.items() if v[1] > 0}
+    line = {"metric": "Euler Gcell-stage-updates/s FP64 swept vs standard (1 B200)",
+            "value": cells / (ms_sw / 1000) / 1e9, "unit": "Gcell-stage-updates/s",
+            "standard": cells / (ms_st / 1000) / 1e9, "swept_ms": ms_sw, "standard_ms": ms_st,
+            "swept_equals_standard": bool(np.array_equal(out_sw, out_st)),
+            "kernel_share": {k: v / sum(kinds.values()) for k, v in kinds.items()},
+            "n": n, "time_steps": steps, "blocksize": bs, "stages_per_step": 2,
+            "dtype": "f64", "data": "synthetic", "steps": args.steps}
+    print(json.dumps(line), flush=True)
+    eng.close()
     return 0
 
 
@@ -639,11 +717,18 @@ def main():
     ap.add_argument("--ref-n", type=int, default=2048)
     ap.add_argument("--ref-cycles", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--f32", action="store_true",
+                    help="float32 fields (the reference's dtype: float32) on one GPU")
     ap.add_argument("--batched", action="store_true",
                     help="batched instances vs one solver per instance (separate JSON line)")
     ap.add_argument("--batched-steps", type=int, default=1000)
     ap.add_argument("--batch-heat", type=int, default=256)
     ap.add_argument("--batch-euler", type=int, default=64)
+    ap.add_argument("--euler", action="store_true",
+                    help="Euler swept vs standard (separate JSON line)")
+    ap.add_argument("--euler-n", type=int, default=4096)
+    ap.add_argument("--euler-steps", type=int, default=1000)
+    ap.add_argument("--euler-bs", type=int, default=32)
     ap.add_argument("--adjoint", action="store_true",
                     help="inverse heat problem: adjoint vs forward cost (separate JSON line)")
     ap.add_argument("--adj-n", type=int, default=2048)
@@ -658,6 +743,8 @@ def main():
         return run_batched(args)
     if args.adjoint:
         return run_adjoint(args)
+    if args.euler:
+        return run_euler(args)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:
         return run_b200_slabs(args)
     return run_b200(args)

@@ -40,6 +40,14 @@ extern "C" {
 #define PS_EQ_CHECKER 3
 #define PS_EQ_HALF 4
 
+/* Storage type of a solver's fields (ps_create_typed).  PS_DTYPE_F32 is the
+ * reference's `dtype: float32` (pysweep/core/io.py:72-73): every level is
+ * stored in float32 and evaluated in float64 (the plugin's constants are
+ * float64 scalars), i.e. rounded to float32 once per level.  Heat with
+ * forward Euler only. */
+#define PS_DTYPE_F64 0
+#define PS_DTYPE_F32 1
+
 /* decompositions (yaml key "swept", pysweep/core/io.py:46) */
 #define PS_MODE_SWEPT 0
 #define PS_MODE_STANDARD 1
@@ -57,6 +65,14 @@ typedef struct ps_solver ps_solver;
  */
 int ps_create(ps_solver **out, int device, int equation, int nv, int nx, int ny, int ops, int its,
               int blocksize);
+
+/* ps_create with the fields' storage type (PS_DTYPE_F64 or PS_DTYPE_F32; the
+ * yaml key `dtype`, pysweep/core/io.py:72-73).  With PS_DTYPE_F32 every
+ * buffer passed to ps_set_state, ps_get_state, ps_get_rows, ps_set_rows and
+ * ps_run's frames holds floats (the `double *` parameters are then read as
+ * `float *`). */
+int ps_create_typed(ps_solver **out, int device, int equation, int nv, int nx, int ny, int ops,
+                    int its, int blocksize, int dtype);
 
 /* Release everything the solver owns.  Replaces process.cleanupProcesses'
  * context pop (pysweep/core/process.py:28-33). */

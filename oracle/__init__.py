@@ -46,6 +46,9 @@ def lib():
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp,
                                    ctypes.c_long, dp, ctypes.c_int]
         L.oracle_max_threads.restype = ctypes.c_int
+        L.oracle_heat_f32.restype = ctypes.c_long
+        L.oracle_heat_f32.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_long, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -128,3 +131,18 @@ def swept(eqn, ic, globals_, its, ops, bs, max_gss=None, nthreads=1, frames=True
 
 def max_threads():
     return lib().oracle_max_threads()
+
+
+def heat_f32(ic, globals_, nlevels, nthreads=1):
+    """Forward-Euler heat with float32 storage: each level is evaluated in
+    float64 (the plugin's courant is a float64 scalar) and rounded to float32,
+    as the reference does with `dtype: float32`.  Returns the final field
+    (float32)."""
+    u = np.ascontiguousarray(ic, dtype=np.float32).copy()
+    _, nx, ny = u.shape
+    courant = params("heat", globals_)[0]
+    got = lib().oracle_heat_f32(u.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), nx, ny,
+                                courant, int(nlevels), nthreads)
+    if got < 0:
+        raise RuntimeError("oracle_heat_f32 failed")
+    return u

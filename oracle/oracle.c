@@ -564,3 +564,39 @@ int oracle_max_threads(void)
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------ heat, float32 -- */
+/* The reference run with `dtype: float32` (io.py:72-73) keeps every level in
+ * a float32 array, but heat.py's courant (heat.py:37) is a float64 scalar, so
+ * numpy evaluates each step in float64 and rounds the result to float32 when
+ * it is stored: u_{n+1} = float32(heat_fe_64(u_n)).  Forward Euler only.
+ * Pinned against the reference's float32 standard frames
+ * (tests/golden/heat_fe_f32_*.npz). */
+long oracle_heat_f32(float *u, int nx, int ny, double courant, long nlevels, int nthreads)
+{
+    size_t n = (size_t)nx * ny;
+    float *tmp = (float *)malloc(n * sizeof(float));
+    if (!tmp) return -1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    for (long L = 0; L < nlevels; ++L) {
+#pragma omp parallel for schedule(static)
+        for (int x = 0; x < nx; ++x) {
+            const float *r = u + (size_t)x * ny;
+            const float *up = u + (size_t)((x + nx - 1) % nx) * ny;
+            const float *dn = u + (size_t)((x + 1) % nx) * ny;
+            for (int y = 0; y < ny; ++y) {
+                double c = r[y];
+                double dx2 = courant * (((double)dn[y] - 2.0 * c) + (double)up[y]);
+                double dy2 = courant * (((double)r[(y + 1) % ny] - 2.0 * c) + (double)r[(y + ny - 1) % ny]);
+                tmp[(size_t)x * ny + y] = (float)((dx2 + dy2) + c);
+            }
+        }
+        memcpy(u, tmp, n * sizeof(float));
+    }
+    free(tmp);
+    return nlevels;
+}

@@ -22,7 +22,9 @@
 // one halo row above and below the strip and one halo column either side, so
 // the second step finds its neighbours in registers.  Every cell sees the
 // same operations in the same order as in the one-step kernels, so fused and
-// unfused passes agree bitwise.
+// unfused passes agree bitwise.  Operand rows reach each warp through a
+// cp.async ring in shared memory three rows ahead of use (RowRing), which
+// keeps enough loads in flight at the occupancy the register use allows.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -160,43 +162,126 @@ __global__ void courant_kernel(const double* __restrict__ alpha, double* __restr
         C[i] = alpha[i] * dt / dx / dx;
 }
 
-// u' = (C*dxx + C*dyy) + u
+// ---- operand rings ---------------------------------------------------------
+// Every kernel below streams a strip down its rows; iteration t needs a few
+// rows of its operands.  A warp copies them with cp.async into a ring of
+// kRingSlots slots kRingDepth iterations before they are used, so loads stay
+// in flight without holding registers.  A slot holds P 16-byte pairs per lane
+// ([P][32 lanes][2]) and HH halo values for the edge lanes 0 and 31
+// ([HH][2]).  Each lane reads back only what it copied; a slot is refilled
+// one iteration after it was read.
+constexpr int kRingDepth = 3;
+constexpr int kRingSlots = kRingDepth + 1;
+
+template <int P, int HH>
+struct RowRing {
+    static constexpr int kSlot = P * 64 + HH * 2;  // doubles per slot
+    static constexpr size_t smem(int warps) { return sizeof(double) * warps * kRingSlots * kSlot; }
+    double* base;
+    int lane, edge;  // edge: 0 for lane 0, 1 for lane 31
+    __device__ RowRing(double* sm, const Strip& s)
+        : base(sm + (threadIdx.x >> 5) * kRingSlots * kSlot), lane(s.lane), edge(s.lane == 31)
+    {
+    }
+    __device__ double* slot(int t) const { return base + (t % kRingSlots) * kSlot; }
+    __device__ void pair(double* sl, int f, const double* src) const
+    {
+        cp_async16(sl + (f * 32 + lane) * 2, src);
+    }
+    __device__ void halo(double* sl, int h, const double* src) const
+    {
+        cp_async8(sl + P * 64 + h * 2 + edge, src);
+    }
+    __device__ double2 get_pair(const double* sl, int f) const
+    {
+        return *reinterpret_cast<const double2*>(sl + (f * 32 + lane) * 2);
+    }
+    __device__ double get_halo(const double* sl, int h, bool on) const
+    {
+        return on ? sl[P * 64 + h * 2 + edge] : 0.0;
+    }
+};
+
+// u' = (C*dxx + C*dyy) + u.  Iteration x (rows x0 .. xend-1): u row x+1, C row x.
 __global__ void __launch_bounds__(256) heatvar_step(const double* __restrict__ u,
                                                     const double* __restrict__ C,
                                                     double* __restrict__ out, int nx, int ny,
                                                     int rows)
 {
+    extern __shared__ double ring_sm[];
     const Strip s(nx, ny, rows);
     if (!s.active()) return;
+    using Ring = RowRing<2, 1>;
+    const Ring R(ring_sm, s);
+    const int n = s.xend - s.x0;
+    auto issue = [&](int t) {
+        if (t < n) {
+            double* sl = R.slot(t);
+            const size_t r1 = s.row(s.x0 + t + 1);
+            R.pair(sl, 0, u + r1 + s.g);
+            R.pair(sl, 1, C + s.row(s.x0 + t) + s.g);
+            if (s.edge()) R.halo(sl, 0, u + r1 + s.hcol);
+        }
+        cp_async_commit();
+    };
+    for (int t = 0; t < kRingDepth; ++t) issue(t);
     Row up = load_row(u, s, s.x0 - 1), ce = load_row(u, s, s.x0);
-    for (int x = s.x0; x < s.xend; ++x) {
-        const Row dn = load_row(u, s, x + 1);
-        const double2 cr = *reinterpret_cast<const double2*>(C + s.row(x) + s.g);
+    for (int t = 0; t < n; ++t) {
+        cp_async_wait<kRingDepth - 1>();
+        const double* sl = R.slot(t);
+        const double2 dv = R.get_pair(sl, 0), cr = R.get_pair(sl, 1);
+        const Row dn{dv.x, dv.y, R.get_halo(sl, 0, s.edge())};
+        issue(t + kRingDepth);
         double n0, n1;
         fe_pair(up, ce, dn, cr.x, cr.y, s.lane, n0, n1);
-        store_pair(out, s, x, n0, n1);
+        store_pair(out, s, s.x0 + t, n0, n1);
         up = ce;
         ce = dn;
     }
 }
 
 // Two forward steps: mid = step(u), out = step(mid).  The first step runs on
-// rows x0-1 .. xend and on the halo columns.
+// rows x0-1 .. xend and on the halo columns.  Iteration i = x0-1+t: u row i+1
+// (two halo columns), C row i+1.
 __global__ void __launch_bounds__(256) heatvar_step2(const double* __restrict__ u,
                                                      const double* __restrict__ C,
                                                      double* __restrict__ mid,
                                                      double* __restrict__ out, int nx, int ny,
                                                      int rows)
 {
+    extern __shared__ double ring_sm[];
     const Strip s(nx, ny, rows);
     if (!s.active()) return;
+    using Ring = RowRing<2, 3>;
+    const Ring R(ring_sm, s);
+    const int n = s.xend - s.x0 + 2;  // iterations i = x0-1 .. xend
+    auto issue = [&](int t) {
+        if (t < n) {
+            double* sl = R.slot(t);
+            const size_t r1 = s.row(s.x0 + t);  // row i+1
+            R.pair(sl, 0, u + r1 + s.g);
+            R.pair(sl, 1, C + r1 + s.g);
+            if (s.edge()) {
+                R.halo(sl, 0, u + r1 + s.hcol);
+                R.halo(sl, 1, u + r1 + s.hcol2);
+                R.halo(sl, 2, C + r1 + s.hcol);
+            }
+        }
+        cp_async_commit();
+    };
+    for (int t = 0; t < kRingDepth; ++t) issue(t);
     Row2 uu = load_row2(u, s, s.x0 - 2), uc = load_row2(u, s, s.x0 - 1);
     Row cc = load_row(C, s, s.x0 - 1);
     Row cp{0.0, 0.0, 0.0};  // C one row up (own columns)
     Row mu{0.0, 0.0, 0.0}, mc{0.0, 0.0, 0.0};  // first-step rows i-2, i-1
-    for (int i = s.x0 - 1; i <= s.xend; ++i) {
-        const Row2 ud = load_row2(u, s, i + 1);
-        const Row cn = i < s.xend ? load_row(C, s, i + 1) : Row{0.0, 0.0, 0.0};
+    for (int t = 0; t < n; ++t) {
+        const int i = s.x0 - 1 + t;
+        cp_async_wait<kRingDepth - 1>();
+        const double* sl = R.slot(t);
+        const double2 uv = R.get_pair(sl, 0), cv = R.get_pair(sl, 1);
+        const Row2 ud{uv.x, uv.y, R.get_halo(sl, 0, s.edge()), R.get_halo(sl, 1, s.edge())};
+        const Row cn{cv.x, cv.y, R.get_halo(sl, 2, s.edge())};
+        issue(t + kRingDepth);
         Row m;
         fe_pair(uu.row(), uc.row(), ud.row(), cc.a, cc.b, s.lane, m.a, m.b);
         m.h = fe_halo(uu, uc, ud, cc.h, s.lane);
@@ -215,7 +300,8 @@ __global__ void __launch_bounds__(256) heatvar_step2(const double* __restrict__ 
     }
 }
 
-// One adjoint level: lam_out = lam + L(C .* lam);  gC += lam .* L(u)
+// One adjoint level: lam_out = lam + L(C .* lam);  gC += lam .* L(u).
+// Iteration x: lam, C and u rows x+1 (halo column), lam and gC rows x.
 __global__ void __launch_bounds__(256) heatvar_adjoint(const double* __restrict__ lam,
                                                        const double* __restrict__ C,
                                                        const double* __restrict__ u,
@@ -223,29 +309,52 @@ __global__ void __launch_bounds__(256) heatvar_adjoint(const double* __restrict_
                                                        double* __restrict__ gC, int nx, int ny,
                                                        int rows)
 {
+    extern __shared__ double ring_sm[];
     const Strip s(nx, ny, rows);
     if (!s.active()) return;
-    auto mu_row = [&](int x) {
-        const Row l = load_row(lam, s, x), c = load_row(C, s, x);
-        Row m;
-        m.a = __dmul_rn(c.a, l.a);
-        m.b = __dmul_rn(c.b, l.b);
-        m.h = __dmul_rn(c.h, l.h);
-        return m;
+    using Ring = RowRing<5, 3>;
+    const Ring R(ring_sm, s);
+    const int n = s.xend - s.x0;
+    auto issue = [&](int t) {
+        if (t < n) {
+            double* sl = R.slot(t);
+            const size_t r1 = s.row(s.x0 + t + 1), r0 = s.row(s.x0 + t);
+            R.pair(sl, 0, lam + r1 + s.g);
+            R.pair(sl, 1, C + r1 + s.g);
+            R.pair(sl, 2, u + r1 + s.g);
+            R.pair(sl, 3, lam + r0 + s.g);
+            R.pair(sl, 4, gC + r0 + s.g);
+            if (s.edge()) {
+                R.halo(sl, 0, lam + r1 + s.hcol);
+                R.halo(sl, 1, C + r1 + s.hcol);
+                R.halo(sl, 2, u + r1 + s.hcol);
+            }
+        }
+        cp_async_commit();
     };
-    Row mup = mu_row(s.x0 - 1), mce = mu_row(s.x0);
+    for (int t = 0; t < kRingDepth; ++t) issue(t);
+    auto mu_of = [](const Row& c, const Row& l) {
+        return Row{__dmul_rn(c.a, l.a), __dmul_rn(c.b, l.b), __dmul_rn(c.h, l.h)};
+    };
+    Row mup = mu_of(load_row(C, s, s.x0 - 1), load_row(lam, s, s.x0 - 1));
+    Row mce = mu_of(load_row(C, s, s.x0), load_row(lam, s, s.x0));
     Row uup = load_row(u, s, s.x0 - 1), uce = load_row(u, s, s.x0);
-    for (int x = s.x0; x < s.xend; ++x) {
-        const Row mdn = mu_row(x + 1), udn = load_row(u, s, x + 1);
+    for (int t = 0; t < n; ++t) {
+        const int x = s.x0 + t;
+        cp_async_wait<kRingDepth - 1>();
+        const double* sl = R.slot(t);
+        const double2 lv = R.get_pair(sl, 0), cv = R.get_pair(sl, 1), uv = R.get_pair(sl, 2);
+        const double2 l = R.get_pair(sl, 3), gc = R.get_pair(sl, 4);
+        const Row ldn{lv.x, lv.y, R.get_halo(sl, 0, s.edge())};
+        const Row cdn{cv.x, cv.y, R.get_halo(sl, 1, s.edge())};
+        const Row udn{uv.x, uv.y, R.get_halo(sl, 2, s.edge())};
+        issue(t + kRingDepth);
+        const Row mdn = mu_of(cdn, ldn);
         double lm0, lm1, lu0, lu1;
         lap(mup, mce, mdn, s.lane, lm0, lm1);
         lap(uup, uce, udn, s.lane, lu0, lu1);
-        const size_t o = s.row(x) + s.g;
-        const double2 l = *reinterpret_cast<const double2*>(lam + o);
-        const double2 gc = *reinterpret_cast<const double2*>(gC + o);
-        *reinterpret_cast<double2*>(lam_out + o) = make_double2(__dadd_rn(l.x, lm0), __dadd_rn(l.y, lm1));
-        *reinterpret_cast<double2*>(gC + o) =
-            make_double2(__fma_rn(l.x, lu0, gc.x), __fma_rn(l.y, lu1, gc.y));
+        store_pair(lam_out, s, x, __dadd_rn(l.x, lm0), __dadd_rn(l.y, lm1));
+        store_pair(gC, s, x, __fma_rn(l.x, lu0, gc.x), __fma_rn(l.y, lu1, gc.y));
         mup = mce;
         mce = mdn;
         uup = uce;
@@ -257,14 +366,41 @@ __global__ void __launch_bounds__(256) heatvar_adjoint(const double* __restrict_
 //     lambda_n     = lam + L(C .* lam)            (rows x0-1 .. xend, halo columns)
 //     lambda_{n-1} = lambda_n + L(C .* lambda_n)  -> lam_out
 //     gC += lam .* L(u_hi);  gC += lambda_n .* L(u_lo)   (one read, one write)
-// Iteration i evaluates the first level at row i and the second at row i-1.
+// Iteration i = x0-1+t evaluates the first level at row i and the second at
+// row i-1; it needs lam, C, u_hi rows i+1 and u_lo, gC rows i.  (gC row i is
+// written one iteration after it is read, by this warp only.)
 __global__ void __launch_bounds__(256) heatvar_adjoint2(
     const double* __restrict__ lam, const double* __restrict__ C, const double* __restrict__ u_hi,
     const double* __restrict__ u_lo, double* __restrict__ lam_out, double* __restrict__ gC, int nx,
     int ny, int rows)
 {
+    extern __shared__ double ring_sm[];
     const Strip s(nx, ny, rows);
     if (!s.active()) return;
+    using Ring = RowRing<5, 6>;
+    const Ring R(ring_sm, s);
+    const int n = s.xend - s.x0 + 2;  // iterations i = x0-1 .. xend
+    auto issue = [&](int t) {
+        if (t < n) {
+            double* sl = R.slot(t);
+            const size_t r1 = s.row(s.x0 + t), r0 = s.row(s.x0 - 1 + t);  // rows i+1, i
+            R.pair(sl, 0, lam + r1 + s.g);
+            R.pair(sl, 1, C + r1 + s.g);
+            R.pair(sl, 2, u_hi + r1 + s.g);
+            R.pair(sl, 3, u_lo + r0 + s.g);
+            R.pair(sl, 4, gC + r0 + s.g);
+            if (s.edge()) {
+                R.halo(sl, 0, lam + r1 + s.hcol);
+                R.halo(sl, 1, lam + r1 + s.hcol2);
+                R.halo(sl, 2, C + r1 + s.hcol);
+                R.halo(sl, 3, C + r1 + s.hcol2);
+                R.halo(sl, 4, u_hi + r1 + s.hcol);
+                R.halo(sl, 5, u_lo + r0 + s.hcol);
+            }
+        }
+        cp_async_commit();
+    };
+    for (int t = 0; t < kRingDepth; ++t) issue(t);
     Row2 lc = load_row2(lam, s, s.x0 - 1), cc = load_row2(C, s, s.x0 - 1);
     Row2 m1u = mul_row2(load_row2(C, s, s.x0 - 2), load_row2(lam, s, s.x0 - 2));
     Row2 m1c = mul_row2(cc, lc);
@@ -273,8 +409,18 @@ __global__ void __launch_bounds__(256) heatvar_adjoint2(
     Row m0u{0.0, 0.0, 0.0}, m0c{0.0, 0.0, 0.0};  // C .* lambda_n, rows i-2, i-1
     double ln0 = 0.0, ln1 = 0.0;                  // lambda_n at row i-1
     double g0 = 0.0, g1 = 0.0;                    // gC after the first level, row i-1
-    for (int i = s.x0 - 1; i <= s.xend; ++i) {
-        const Row2 ld = load_row2(lam, s, i + 1), cd = load_row2(C, s, i + 1);
+    for (int t = 0; t < n; ++t) {
+        const int i = s.x0 - 1 + t;
+        cp_async_wait<kRingDepth - 1>();
+        const double* sl = R.slot(t);
+        const bool e = s.edge();
+        const double2 lv = R.get_pair(sl, 0), cv = R.get_pair(sl, 1), hv = R.get_pair(sl, 2);
+        const double2 wv = R.get_pair(sl, 3), gold = R.get_pair(sl, 4);
+        const Row2 ld{lv.x, lv.y, R.get_halo(sl, 0, e), R.get_halo(sl, 1, e)};
+        const Row2 cd{cv.x, cv.y, R.get_halo(sl, 2, e), R.get_halo(sl, 3, e)};
+        const Row hd{hv.x, hv.y, R.get_halo(sl, 4, e)};
+        const Row ldn{wv.x, wv.y, R.get_halo(sl, 5, e)};
+        issue(t + kRingDepth);
         const Row2 m1d = mul_row2(cd, ld);
         // first level at row i
         double a0, a1;
@@ -284,10 +430,8 @@ __global__ void __launch_bounds__(256) heatvar_adjoint2(
         const Row m0{__dmul_rn(cc.a, ln.a), __dmul_rn(cc.b, ln.b), __dmul_rn(cc.h, ln.h)};
         double ng0 = 0.0, ng1 = 0.0;
         if (i >= s.x0 && i < s.xend) {
-            const Row hd = load_row(u_hi, s, i + 1);
             double q0, q1;
             lap(hu, hc, hd, s.lane, q0, q1);
-            const double2 gold = *reinterpret_cast<const double2*>(gC + s.row(i) + s.g);
             ng0 = __fma_rn(lc.a, q0, gold.x);
             ng1 = __fma_rn(lc.b, q1, gold.y);
             hu = hc;
@@ -295,7 +439,6 @@ __global__ void __launch_bounds__(256) heatvar_adjoint2(
         }
         // second level at row i-1
         if (i > s.x0) {
-            const Row ldn = load_row(u_lo, s, i);
             double b0, b1, q0, q1;
             lap(m0u, m0c, m0, s.lane, b0, b1);
             lap(lu, lcur, ldn, s.lane, q0, q1);
@@ -324,19 +467,36 @@ __global__ void scale_kernel(double* __restrict__ g, size_t n, double f)
         g[i] *= f;
 }
 
-// Rows per strip: 32, halved while the grid has fewer than about 24 warps per
-// SM of a 148-SM part (the kernels stream rows one after the other, so small
-// grids need more, shorter strips to keep loads in flight).
-int adj_rows(int nx, int ny)
+// Rows per strip: 64, halved (down to 8) while the grid has fewer warps than
+// `per_sm` per SM of a 148-SM part.  Each kernel streams its strip row after
+// row, so a kernel that fits many warps per SM (few registers) wants many
+// short strips, one with few warps per SM wants tall strips (less halo work).
+int adj_rows(int nx, int ny, int per_sm)
 {
-    int rows = 32;
-    while (rows > 8 && (long long)(ny / 64) * ((nx + rows - 1) / rows) < 148LL * 24) rows /= 2;
+    int rows = 64;
+    while (rows > 8 && (long long)(ny / 64) * ((nx + rows - 1) / rows) < 148LL * per_sm) rows /= 2;
     return rows;
 }
 
 dim3 strip_grid(int nx, int ny, int rows)
 {
     return dim3((ny / 64 + 7) / 8, (nx + rows - 1) / rows);
+}
+
+// shared memory of the ring-fed kernels (8 warps per CTA)
+constexpr size_t kStepSmem = RowRing<2, 1>::smem(8);
+constexpr size_t kStep2Smem = RowRing<2, 3>::smem(8);
+constexpr size_t kAdjSmem = RowRing<5, 3>::smem(8);
+constexpr size_t kAdj2Smem = RowRing<5, 6>::smem(8);
+
+cudaError_t allow_ring_smem()
+{
+    cudaError_t e = cudaFuncSetAttribute(heatvar_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kAdjSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(heatvar_adjoint2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kAdj2Smem);
+    return e;
 }
 
 }  // namespace
@@ -375,7 +535,7 @@ extern "C" int ps_heatvar_forward(const double* d_u0, const double* d_alpha, dou
     }
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)nx * ny;
-    const int rows = adj_rows(nx, ny);
+    const int rows = adj_rows(nx, ny, 48);  // heatvar_step: 40 registers
     courant_kernel<<<1024, 256, 0, st>>>(d_alpha, d_courant, n, dt, dx);
     // ping-pong between d_work and d_uT so that the last step lands in d_uT
     const double* in = d_u0;
@@ -388,7 +548,8 @@ extern "C" int ps_heatvar_forward(const double* d_u0, const double* d_alpha, dou
                         err, errlen);
     for (int64_t k = 0; k < nsteps; ++k) {
         double* out = ((nsteps - 1 - k) % 2 == 0) ? d_uT : d_work;
-        heatvar_step<<<strip_grid(nx, ny, rows), 256, 0, st>>>(in, d_courant, out, nx, ny, rows);
+        heatvar_step<<<strip_grid(nx, ny, rows), 256, kStepSmem, st>>>(in, d_courant, out, nx, ny,
+                                                                       rows);
         if (d_checkpoints && (k + 1) % every == 0 && k + 1 < nsteps)
             if ((rc = adj_cuda(cudaMemcpyAsync(d_checkpoints + (size_t)((k + 1) / every) * n, out,
                                                n * sizeof(double), cudaMemcpyDeviceToDevice, st),
@@ -413,9 +574,13 @@ extern "C" int ps_heatvar_adjoint(const double* d_courant, const double* d_check
     }
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)nx * ny;
-    const int rows = adj_rows(nx, ny);
-    const dim3 grid = strip_grid(nx, ny, rows);
+    const int rows = adj_rows(nx, ny, 8);      // heatvar_step2: 80 registers
+    const int rows_a = adj_rows(nx, ny, 8);    // heatvar_adjoint2: 128 registers
+    const int rows_1 = adj_rows(nx, ny, 16);   // heatvar_step, heatvar_adjoint
+    const dim3 grid = strip_grid(nx, ny, rows), grid_a = strip_grid(nx, ny, rows_a);
+    const dim3 grid_1 = strip_grid(nx, ny, rows_1);
     const int64_t nseg = (nsteps + every - 1) / every;
+    if ((rc = adj_cuda(allow_ring_smem(), err, errlen))) return rc;
     // adjoint launches: two levels per launch, one more for an odd segment
     int64_t launches = 0;
     for (int64_t sidx = 0; sidx < nseg; ++sidx) {
@@ -438,25 +603,25 @@ extern "C" int ps_heatvar_adjoint(const double* d_courant, const double* d_check
             return rc;
         int64_t j = 1;
         for (; j + 1 < len; j += 2)
-            heatvar_step2<<<grid, 256, 0, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
+            heatvar_step2<<<grid, 256, kStep2Smem, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
                                                 d_states + (size_t)j * n,
                                                 d_states + (size_t)(j + 1) * n, nx, ny, rows);
         if (j < len)
-            heatvar_step<<<grid, 256, 0, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
-                                               d_states + (size_t)j * n, nx, ny, rows);
+            heatvar_step<<<grid_1, 256, kStepSmem, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
+                                                         d_states + (size_t)j * n, nx, ny, rows_1);
         // adjoint levels k = len-1 .. 0 of the segment (lambda_{n0+k+1} -> lambda_{n0+k})
         int64_t k = len - 1;
         for (; k >= 1; k -= 2) {
             double* out = lam == d_lam0 ? d_lamwork : d_lam0;
-            heatvar_adjoint2<<<grid, 256, 0, st>>>(lam, d_courant, d_states + (size_t)k * n,
-                                                   d_states + (size_t)(k - 1) * n, out, d_galpha,
-                                                   nx, ny, rows);
+            heatvar_adjoint2<<<grid_a, 256, kAdj2Smem, st>>>(lam, d_courant, d_states + (size_t)k * n,
+                                                     d_states + (size_t)(k - 1) * n, out,
+                                                     d_galpha, nx, ny, rows_a);
             lam = out;
         }
         if (k == 0) {
             double* out = lam == d_lam0 ? d_lamwork : d_lam0;
-            heatvar_adjoint<<<grid, 256, 0, st>>>(lam, d_courant, d_states, out, d_galpha, nx, ny,
-                                                  rows);
+            heatvar_adjoint<<<grid_1, 256, kAdjSmem, st>>>(lam, d_courant, d_states, out, d_galpha,
+                                                           nx, ny, rows_1);
             lam = out;
         }
     }

@@ -61,6 +61,28 @@ struct Heat {
     }
 };
 
+// Heat, forward Euler, on float32 fields: the reference run with
+// `dtype: float32` (pysweep/core/io.py:72-73) stores every level in float32,
+// while heat.py's courant is a float64 scalar, so numpy evaluates the step in
+// float64 (the order above) and rounds the result to float32 on store.
+struct HeatF32 {
+    static constexpr int OPS = 1;
+    static constexpr int ID = EQ_HEAT;
+    __device__ static __forceinline__ void step(const float* __restrict__ u,
+                                                const float* __restrict__ up,
+                                                float* __restrict__ o, const Nbr& n, int gts,
+                                                int nv, const EqParams& p)
+    {
+        const double c = u[0];
+        const double cr = p.d[0];
+        const double dxx = __dmul_rn(cr, __dadd_rn(__fma_rn(-2.0, c, (double)u[n.x[3]]),
+                                                   (double)u[n.x[1]]));
+        const double dyy = __dmul_rn(cr, __dadd_rn(__fma_rn(-2.0, c, (double)u[n.y[3]]),
+                                                   (double)u[n.y[1]]));
+        o[0] = __double2float_rn(__dadd_rn(__dadd_rn(dxx, dyy), c));
+    }
+};
+
 // half.py: (u[x+1]-2u+u[x-1])/100 + (u[y+1]-2u+u[y-1])/100, RK2 on gts%2
 struct Half {
     static constexpr int OPS = 1;

@@ -19,10 +19,10 @@
 //     early exit.  The gap (XBridge) keeps level m-1's rows [hx-m-1, hx+m+1)
 //     (two face rows of the upper prism, its own rows, two face rows of the
 //     lower prism) at indices [0, 2m+2) and updates them in place in
-//     descending order, entering at the level's first row through a switch
-//     (Duff's device).  Each gap row computes its own left neighbours from
-//     the arrays and the carry, so no value travels from one row to the next
-//     and the entry points cost no register moves.
+//     descending order, two rows at a time, entering at the level's first
+//     row pair through a switch (Duff's device).  Each row pair computes its
+//     left neighbours from the arrays and the carry, so no value travels from
+//     one pair to the next and the entry points cost no register moves.
 //
 // Per cell: 8 FP64 operations (numpy's operation order, see Heat in
 // equations.cuh) and one (prism) or two (gap) 64-bit shuffles.  Shared memory
@@ -46,18 +46,64 @@ __device__ __forceinline__ double heat_fe(double c, double xm, double xp, double
     return __dadd_rn(__dadd_rn(dxx, dyy), c);
 }
 
+// Storage type of the fields.  double; or float, every level evaluated in
+// double and rounded to float (the reference's float32 runs: its courant is a
+// float64 scalar, so numpy computes each level in float64 and rounds it when
+// it is stored).  Registers, carry and arithmetic are double in both cases.
+template <class T>
+struct Pair2;
+template <>
+struct Pair2<double> {
+    using type = double2;
+};
+template <>
+struct Pair2<float> {
+    using type = float2;
+};
+
+template <class T>
+__device__ __forceinline__ double to_level(double x)
+{
+    return x;
+}
+template <>
+__device__ __forceinline__ double to_level<float>(double x)
+{
+    return (double)__double2float_rn(x);
+}
+
+template <class T>
+__device__ __forceinline__ typename Pair2<T>::type pair2(double x, double y);
+template <>
+__device__ __forceinline__ double2 pair2<double>(double x, double y)
+{
+    return make_double2(x, y);
+}
+template <>
+__device__ __forceinline__ float2 pair2<float>(double x, double y)
+{
+    return make_float2((float)x, (float)y);  // exact: x, y already carry float precision
+}
+
+template <class P>
+__device__ __forceinline__ double2 widen(P v)
+{
+    return make_double2((double)v.x, (double)v.y);
+}
+
 // A lane's column pair starts on an even column at even levels and on an odd
 // column at odd levels (the chunk shifts one column per level); 16-byte
 // vector stores are only legal in the even case (`even` is warp-uniform).
 // In the odd case the pair may straddle the periodic column boundary, so the
 // second column index g1 is wrapped separately.
-__device__ __forceinline__ void st_pair(double* row, int g, int g1, double x, double y, bool even)
+template <class T>
+__device__ __forceinline__ void st_pair(T* row, int g, int g1, double x, double y, bool even)
 {
     if (even) {
-        *reinterpret_cast<double2*>(row + g) = make_double2(x, y);
+        *reinterpret_cast<typename Pair2<T>::type*>(row + g) = pair2<T>(x, y);
     } else {
-        row[g] = x;
-        row[g1] = y;
+        row[g] = (T)x;
+        row[g1] = (T)y;
     }
 }
 
@@ -102,17 +148,27 @@ constexpr size_t heat_fast_smem(int hmax)
 // 16-byte global -> shared copies that complete asynchronously (cp.async,
 // one commit group per level; wait_group<N> waits until at most N groups of
 // this thread are still in flight)
-__device__ __forceinline__ void cp_async16(double* smem, const double* gmem)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
 // 8-byte copy (cp.async.ca: the 4- and 8-byte sizes go through L1)
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// one pair of T (16 bytes for double, 8 for float)
+template <class T>
+__device__ __forceinline__ void cp_async_pair(T* smem, const T* gmem)
+{
+    if constexpr (sizeof(T) == 8)
+        cp_async16(smem, gmem);
+    else
+        cp_async8(smem, gmem);
 }
 
 __device__ __forceinline__ void cp_async_commit()
@@ -129,27 +185,31 @@ __device__ __forceinline__ void cp_async_wait()
 // A new cell pair from this lane's old rows (up u0, centre c0/c1, down d0)
 // and the left neighbour's values (column 1 at up / centre / down rows L1u,
 // L1c, L1d; column 0 at the centre row L0c).
+// The results are rounded to the storage precision of T.
+template <class T = double>
 __device__ __forceinline__ void heat_pair(double L1u, double L1c, double L1d, double L0c,
                                           double u0, double c0, double d0, double c1, double cr,
                                           double& n0, double& n1)
 {
-    n0 = heat_fe(L1c, L1u, L1d, L0c, c0, cr);
-    n1 = heat_fe(c0, u0, d0, L1c, c1, cr);
+    n0 = to_level<T>(heat_fe(L1c, L1u, L1d, L0c, c0, cr));
+    n1 = to_level<T>(heat_fe(c0, u0, d0, L1c, c1, cr));
 }
 
 // Gap: start the copy of the four prism face rows of level m at this lane's
 // column pair (upper prism's bottom face rows, then lower prism's top face
 // rows) into one ring slot; gcol is the chunk's level-0 column of the lane.
+template <class T>
 __device__ __forceinline__ void issue_faces(const SweptArgs& a, int bup, int band, int HF, int m,
-                                            int gcol, int lane, double* slot)
+                                            int gcol, int lane, T* slot)
 {
+    const T* xface = reinterpret_cast<const T*>(a.xface);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int side = q < 2 ? 1 : 0;
         const int j = q & 1;
         const int bb = q < 2 ? bup : band;
         const size_t fo = (((size_t)bb * HF + (m - 1)) * 2 + side) * 2 + j;
-        cp_async16(slot + (q * 32 + lane) * 2, a.xface + fo * a.ny + gcol);
+        cp_async_pair<T>(slot + (q * 32 + lane) * 2, xface + fo * a.ny + gcol);
     }
 }
 
@@ -186,15 +246,16 @@ __device__ __forceinline__ void place_lower(int m, double2 f2, double2 f3, doubl
 #define PSB_BOTTOM_CASE(C)                                                                 \
     case C:                                                                                \
         if constexpr ((C) <= BX) {                                                         \
-            *reinterpret_cast<double2*>(r0) = make_double2(a0[(C) - 2], a1[(C) - 2]);      \
-            *reinterpret_cast<double2*>(r1) = make_double2(a0[(C) - 1], a1[(C) - 1]);      \
+            *reinterpret_cast<P*>(r0) = pair2<T>(a0[(C) - 2], a1[(C) - 2]);                \
+            *reinterpret_cast<P*>(r1) = pair2<T>(a0[(C) - 1], a1[(C) - 1]);                \
         }                                                                                  \
         break;
 
-template <int BX>
+template <int BX, class T>
 __device__ __forceinline__ void store_bottom(int count, const double (&a0)[BX],
-                                             const double (&a1)[BX], double* r0, double* r1)
+                                             const double (&a1)[BX], T* r0, T* r1)
 {
+    using P = typename Pair2<T>::type;
     static_assert(BX <= 32, "cases cover blocksizes up to 32");
     switch (count) {
         PSB_BOTTOM_CASE(2) PSB_BOTTOM_CASE(4) PSB_BOTTOM_CASE(6) PSB_BOTTOM_CASE(8)
@@ -206,14 +267,14 @@ __device__ __forceinline__ void store_bottom(int count, const double (&a0)[BX],
 }
 #undef PSB_BOTTOM_CASE
 
-// Gap: row K of level m from old rows K-2 (up), K-1 (centre), K (down) and
-// their carried left columns; self-contained, so that no value travels from
-// one row to the next (rows are entered at the level's first row).
-template <int K, int BX>
-__device__ __forceinline__ void gap_row(double (&a0)[BX], double (&a1)[BX], const double* cr0,
-                                        int lane, double cr)
+// Gap: rows K and K-1 of level m (K odd).  Row K takes its left neighbours
+// from the arrays and the carry; row K-1 reuses two of them (the old rows
+// K-2 and K-1 are not written by row K), so a pair needs six shuffles.
+template <int K, int BX, class T>
+__device__ __forceinline__ void gap_pair(double (&a0)[BX], double (&a1)[BX], const double* cr0,
+                                         int lane, double cr)
 {
-    if constexpr (K >= 2 && K < BX) {
+    if constexpr (K >= 3 && K < BX) {
         const double2 cu = *reinterpret_cast<const double2*>(cr0 + (K - 2) * 2);
         const double2 cc = *reinterpret_cast<const double2*>(cr0 + (K - 1) * 2);
         const double2 cd = *reinterpret_cast<const double2*>(cr0 + K * 2);
@@ -222,17 +283,27 @@ __device__ __forceinline__ void gap_row(double (&a0)[BX], double (&a1)[BX], cons
         const double L1d = from_left(a1[K], cd.y, lane);
         const double L0c = from_left(a0[K - 1], cc.x, lane);
         double n0, n1;
-        heat_pair(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], cr, n0, n1);
+        heat_pair<T>(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], cr, n0, n1);
         a0[K] = n0;
         a1[K] = n1;
+        // row K-1: up K-3, centre K-2, down K-1
+        const double2 cuu = *reinterpret_cast<const double2*>(cr0 + (K - 3) * 2);
+        const double L1uu = from_left(a1[K - 3], cuu.y, lane);
+        const double L0cc = from_left(a0[K - 2], cu.x, lane);
+        heat_pair<T>(L1uu, L1u, L1c, L0cc, a0[K - 3], a0[K - 2], a0[K - 1], a1[K - 2], cr, n0,
+                     n1);
+        a0[K - 1] = n0;
+        a1[K - 1] = n1;
     }
 }
 
 // One (band, segment) unit of one warp; `carry` is the warp's own shared
 // memory (heat_fast_warp_doubles: two packed carry buffers, then the ring).
-template <int BX, bool GAP>
+// T: storage type of the fields and faces (double or float).
+template <int BX, bool GAP, class T = double>
 __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int unit, double* carry)
 {
+    using P = typename Pair2<T>::type;
     constexpr int hx = BX / 2;
     const int lane = threadIdx.x & 31;
     const int H = a.H, Hm = a.Hmax, nx = a.nx, ny = a.ny;
@@ -249,7 +320,7 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
     const int CB = 2 * (carry_rows<BX, false>(Hm) > carry_rows<BX, true>(Hm)
                             ? carry_rows<BX, false>(Hm)
                             : carry_rows<BX, true>(Hm));
-    double* ring = carry + 2 * CB;  // gap: [kFaceSlots][4][32][2]
+    T* ring = reinterpret_cast<T*>(carry + 2 * CB);  // gap: [kFaceSlots][4][32][2] of T
     const int HF = Hm - 1;
     const int bup = wrap(band - 1, a.nb);
     const int r0w = wrap(r0, nx);
@@ -264,7 +335,7 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
         const int gcol = wrap(cw + 2 * lane, ny);  // the lane's level-0 column (x-face column)
         // ---- level 0 ------------------------------------------------------
         {
-            const double* b = a.bin;  // its = 1: the only base level
+            const T* b = reinterpret_cast<const T*>(a.bin);  // its = 1: the only base level
             const int g = wrap(cw + 2 * lane, ny);
             auto rowp = [&](int r) {  // band row r, wrapped
                 int row = r0w + r;
@@ -274,19 +345,19 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
             if (!GAP) {
 #pragma unroll
                 for (int i = 0; i < BX; ++i) {
-                    const double2 v = *reinterpret_cast<const double2*>(rowp(i) + g);
+                    const double2 v = widen(*reinterpret_cast<const P*>(rowp(i) + g));
                     a0[i] = v.x;
                     a1[i] = v.y;
                 }
             } else {
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
-                    const double2 v = *reinterpret_cast<const double2*>(rowp(hx - 2 + k) + g);
+                    const double2 v = widen(*reinterpret_cast<const P*>(rowp(hx - 2 + k) + g));
                     a0[k] = v.x;
                     a1[k] = v.y;
                 }
-                const double2 v0 = *reinterpret_cast<const double2*>(rowp(hx) + g);
-                const double2 v1 = *reinterpret_cast<const double2*>(rowp(hx + 1) + g);
+                const double2 v0 = widen(*reinterpret_cast<const P*>(rowp(hx) + g));
+                const double2 v1 = widen(*reinterpret_cast<const P*>(rowp(hx + 1) + g));
                 a0[2] = v0.x;
                 a1[2] = v0.y;
                 a0[3] = v1.x;
@@ -297,7 +368,7 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
             const int rbase = GAP ? hx - 2 : 0;
             const int gl = wrap(cw - 2, ny), gl1 = wrap(cw - 1, ny);
             for (int k = lane; k < nrow0; k += 32) {
-                const double* src = rowp(rbase + k);
+                const T* src = rowp(rbase + k);
                 cin[k * 2 + 0] = src[gl];
                 cin[k * 2 + 1] = src[gl1];
             }
@@ -337,8 +408,8 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                     const double L1d = from_left(a1[i + 2], cd.y, lane);
                     const double L0c = from_left(a0[i + 1], cc.x, lane);
                     double n0, n1;
-                    heat_pair(L1u, L1c, L1d, L0c, a0[i], a0[i + 1], a0[i + 2], a1[i + 1], cr, n0,
-                              n1);
+                    heat_pair<T>(L1u, L1c, L1d, L0c, a0[i], a0[i + 1], a0[i + 2], a1[i + 1], cr,
+                                 n0, n1);
                     a0[i] = n0;
                     a1[i] = n1;
                     L1u = L1c;
@@ -356,64 +427,49 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                 // rows K0 .. 2, entered at K0 = 2m+1 and falling through
                 switch (K0) {
                 case 31:
-                    gap_row<31, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<30, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<31, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 29:
-                    gap_row<29, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<28, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<29, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 27:
-                    gap_row<27, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<26, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<27, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 25:
-                    gap_row<25, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<24, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<25, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 23:
-                    gap_row<23, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<22, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<23, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 21:
-                    gap_row<21, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<20, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<21, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 19:
-                    gap_row<19, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<18, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<19, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 17:
-                    gap_row<17, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<16, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<17, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 15:
-                    gap_row<15, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<14, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<15, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 13:
-                    gap_row<13, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<12, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<13, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 11:
-                    gap_row<11, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<10, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<11, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 9:
-                    gap_row<9, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<8, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<9, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 7:
-                    gap_row<7, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<6, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<7, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 5:
-                    gap_row<5, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<4, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<5, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 case 3:
-                    gap_row<3, BX>(a0, a1, cr0, lane, cr);
-                    gap_row<2, BX>(a0, a1, cr0, lane, cr);
+                    gap_pair<3, BX, T>(a0, a1, cr0, lane, cr);
                     [[fallthrough]];
                 default:
                     break;
@@ -423,17 +479,16 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                 // Each lane reads back only the pairs it copied.
                 if (m <= H - 1) {
                     cp_async_wait<kFaceDepth - 1>();  // level m's group has landed
-                    const double* sl = ring + (m % kFaceSlots) * 256 + lane * 2;
-                    const double2 f0 = *reinterpret_cast<const double2*>(sl + 0 * 64);
-                    const double2 f1 = *reinterpret_cast<const double2*>(sl + 1 * 64);
-                    const double2 f2 = *reinterpret_cast<const double2*>(sl + 2 * 64);
-                    const double2 f3 = *reinterpret_cast<const double2*>(sl + 3 * 64);
+                    const T* sl = ring + (m % kFaceSlots) * 256 + lane * 2;
+                    const double2 f0 = widen(*reinterpret_cast<const P*>(sl + 0 * 64));
+                    const double2 f1 = widen(*reinterpret_cast<const P*>(sl + 1 * 64));
+                    const double2 f2 = widen(*reinterpret_cast<const P*>(sl + 2 * 64));
+                    const double2 f3 = widen(*reinterpret_cast<const P*>(sl + 3 * 64));
                     a0[0] = f0.x;
                     a1[0] = f0.y;
                     a0[1] = f1.x;
                     a1[1] = f1.y;
                     place_lower<BX>(m, f2, f3, a0, a1);
-
                     // refill the slot of level m-1 (read one level ago)
                     const int mf = m + kFaceDepth;
                     if (mf <= H - 1)
@@ -459,15 +514,16 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
             if (!GAP && m <= H - 1 && valid) {
                 // faces are stored at the chunk's level-0 columns (xface_col)
                 const size_t fb = ((size_t)band * HF + (m - 1)) * 2;
-                double* xf = a.xface + gcol;
-                *reinterpret_cast<double2*>(xf + ((fb + 0) * 2 + 0) * ny) = make_double2(a0[0], a1[0]);
-                *reinterpret_cast<double2*>(xf + ((fb + 0) * 2 + 1) * ny) = make_double2(a0[1], a1[1]);
-                store_bottom<BX>(BX - 2 * m, a0, a1, xf + ((fb + 1) * 2 + 0) * ny,
-                                 xf + ((fb + 1) * 2 + 1) * ny);
+                T* xf = reinterpret_cast<T*>(a.xface) + gcol;
+                *reinterpret_cast<P*>(xf + ((fb + 0) * 2 + 0) * ny) = pair2<T>(a0[0], a1[0]);
+                *reinterpret_cast<P*>(xf + ((fb + 0) * 2 + 1) * ny) = pair2<T>(a0[1], a1[1]);
+                store_bottom<BX, T>(BX - 2 * m, a0, a1, xf + ((fb + 1) * 2 + 0) * ny,
+                                    xf + ((fb + 1) * 2 + 1) * ny);
             }
             const long long fs = frame_slot(a, a.L0 + m);
             if (m == H || fs >= 0) {
-                double* fr = fs >= 0 ? a.frames + (size_t)fs * nx * ny : nullptr;
+                T* fr = fs >= 0 ? reinterpret_cast<T*>(a.frames) + (size_t)fs * nx * ny : nullptr;
+                T* bo = reinterpret_cast<T*>(a.bout);
 #pragma unroll
                 for (int i = 0; i < BX; ++i) {
                     if (i >= nrow) break;
@@ -475,8 +531,8 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                     int row = r0w + rfirst + i;
                     row -= row >= nx ? nx : 0;
                     const size_t o = (size_t)row * ny;
-                    if (m == H && valid) st_pair(a.bout + o, gm, gm1, a0[i], a1[i], even);
-                    if (fr && valid) st_pair(fr + o, gm, gm1, a0[i], a1[i], even);
+                    if (m == H && valid) st_pair<T>(bo + o, gm, gm1, a0[i], a1[i], even);
+                    if (fr && valid) st_pair<T>(fr + o, gm, gm1, a0[i], a1[i], even);
                 }
             }
             // y-faces at the segment's column edges (read by the seam kernels)
@@ -485,14 +541,14 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                 for (int side = 0; side < 2; ++side) {
                     if ((side == 0 && !first) || (side == 1 && !last)) continue;
                     const int owner = side == 0 ? m : nact - 1;
-                    double* yf = a.yface + (((size_t)unit * 2 + side) * HF + (m - 1)) * BX * 2;
+                    T* yf = reinterpret_cast<T*>(a.yface) +
+                            (((size_t)unit * 2 + side) * HF + (m - 1)) * BX * 2;
 #pragma unroll
                     for (int i = 0; i < BX; ++i) {
                         if (i >= nrow) break;
                         if (i < ibeg) continue;
                         if (lane == owner)
-                            *reinterpret_cast<double2*>(yf + (rfirst + i) * 2) =
-                                make_double2(a0[i], a1[i]);
+                            *reinterpret_cast<P*>(yf + (rfirst + i) * 2) = pair2<T>(a0[i], a1[i]);
                     }
                 }
             }
@@ -501,14 +557,14 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
     }
 }
 
-template <int BX, bool GAP>
+template <int BX, bool GAP, class T = double>
 __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs a)
 {
     extern __shared__ double sm[];
     const int warp = threadIdx.x >> 5;
     const int unit = blockIdx.x * kFastWarps + warp;
     if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
-    heat_fast_body<BX, GAP>(a, unit, sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
+    heat_fast_body<BX, GAP, T>(a, unit, sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
 }  // namespace psb

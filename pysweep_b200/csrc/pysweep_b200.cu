@@ -59,6 +59,8 @@ struct ps_solver {
     int eq = 0;
     int nv = 1, nx = 0, ny = 0, ops = 1, its = 1, bs = 0;
     int mpss = 0;
+    int dtype = PS_DTYPE_F64;
+    size_t esize = sizeof(double);  // bytes per element of every field and face buffer
     // tiling
     int H = 0, nseg = 1, chunk = 32, threads = 128;
     bool nseg_auto = true;  // choose the segment count per run until configured
@@ -132,6 +134,13 @@ int fail(ps_solver* s, int code, const char* fmt, ...)
     } while (0)
 
 size_t field_elems(const ps_solver* s) { return (size_t)s->nv * s->nx * s->ny; }
+// element offsets and sizes in the solver's storage type (double or float;
+// device buffers are kept as double* and addressed in bytes)
+double* at(const ps_solver* s, double* p, size_t elems)
+{
+    return reinterpret_cast<double*>(reinterpret_cast<char*>(p) + elems * s->esize);
+}
+size_t nbytes(const ps_solver* s, size_t elems) { return elems * s->esize; }
 
 int eq_ops(int eq, int ops)
 {
@@ -191,10 +200,10 @@ void launch_stream(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
     k<<<grid, 256, smem, st>>>(a);
 }
 
-template <class Eq, int ITS, bool GAP>
+template <class Eq, int ITS, bool GAP, class T = double>
 void launch_seam(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
 {
-    auto k = seam_kernel<Eq, ITS, GAP, 128>;
+    auto k = seam_kernel<Eq, ITS, GAP, 128, T>;
     allow_big_smem(k);
     k<<<grid, 128, smem, st>>>(a);
 }
@@ -212,10 +221,10 @@ struct SweptSet {
     bool fast = false;
 };
 
-template <int BX, bool GAP>
+template <int BX, bool GAP, class T = double>
 void launch_fast(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
 {
-    auto k = heat_stream_fast<BX, GAP>;
+    auto k = heat_stream_fast<BX, GAP, T>;
     allow_big_smem(k);
     const int units = a.nb * a.nseg;
     k<<<(units + kFastWarps - 1) / kFastWarps, 32 * kFastWarps, smem, st>>>(a);
@@ -331,14 +340,14 @@ int ensure_swept_buffers(ps_solver* s)
         if (s->xface) cudaFree(s->xface);
         s->xface = nullptr;
         s->xface_n = 0;
-        if (xn) PS_CUDA(s, cudaMalloc(&s->xface, xn * sizeof(double)));
+        if (xn) PS_CUDA(s, cudaMalloc(&s->xface, nbytes(s, xn)));
         s->xface_n = xn;
     }
     if (yn > s->yface_n) {
         if (s->yface) cudaFree(s->yface);
         s->yface = nullptr;
         s->yface_n = 0;
-        if (yn) PS_CUDA(s, cudaMalloc(&s->yface, yn * sizeof(double)));
+        if (yn) PS_CUDA(s, cudaMalloc(&s->yface, nbytes(s, yn)));
         s->yface_n = yn;
     }
     return PS_OK;
@@ -347,14 +356,14 @@ int ensure_swept_buffers(ps_solver* s)
 size_t stream_smem(const ps_solver* s)
 {
     const int O2 = 2 * s->ops, RS = s->chunk + O2;
-    return sizeof(double) * ((size_t)(s->its + 1) * s->nv * s->bs * RS +
-                             (size_t)(s->H + 1) * s->nv * s->bs * O2);
+    return s->esize * ((size_t)(s->its + 1) * s->nv * s->bs * RS +
+                       (size_t)(s->H + 1) * s->nv * s->bs * O2);
 }
 
 size_t seam_smem(const ps_solver* s)
 {
     const int TW = 2 * s->ops * (s->H + 1);
-    return sizeof(double) * (size_t)(s->its + 1) * s->nv * s->bs * TW;
+    return s->esize * (size_t)(s->its + 1) * s->nv * s->bs * TW;
 }
 
 int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t frame_cap,
@@ -368,8 +377,19 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     // register-resident streams for heat with forward Euler (the generic
     // seam kernels are shared)
     const bool fwd_euler = make_params(s).i[0] != 0;
-    if (s->eq == PS_EQ_HEAT && s->its == 1 && fwd_euler && s->threads != 256 &&
-        (s->bs == 16 || s->bs == 32) && s->ny % 32 == 0) {
+    if (s->dtype == PS_DTYPE_F32) {
+        // float32 fields: the register streams and the seams in float storage
+        if (!(s->eq == PS_EQ_HEAT && s->its == 1 && fwd_euler && (s->bs == 16 || s->bs == 32) &&
+              s->ny % 32 == 0))
+            return fail(s, PS_ERR_UNSUPPORTED,
+                        "float32 fields: heat, forward Euler, blocksize 16 or 32, ny a multiple of 32");
+        K.fast = true;
+        K.Y = launch_seam<HeatF32, 1, false, float>;
+        K.O = launch_seam<HeatF32, 1, true, float>;
+        K.P = s->bs == 16 ? launch_fast<16, false, float> : launch_fast<32, false, float>;
+        K.G = s->bs == 16 ? launch_fast<16, true, float> : launch_fast<32, true, float>;
+    } else if (s->eq == PS_EQ_HEAT && s->its == 1 && fwd_euler && s->threads != 256 &&
+               (s->bs == 16 || s->bs == 32) && s->ny % 32 == 0) {
         K.fast = true;
         if (s->bs == 16) {
             K.P = launch_fast<16, false>;
@@ -402,7 +422,17 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
             s->nseg = std::max(1, std::min(s->ny / kFastChunk, slots / nb));
             s->nseg = std::max(1, std::min(s->nseg, s->ny / 32));
         } else {
+            // one CTA per (band, segment): the most segments up to about four
+            // CTAs per SM, each dividing ny and at least one chunk and
+            // 2*ops*(h+1) columns wide (narrower segments add seam work)
+            int sms = 148;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+            const int nb = s->nx / s->bs;
+            const int want = std::max(1, (4 * sms + nb - 1) / nb);
+            const int minw = std::max(s->chunk, O2 * (s->H + 1));
             s->nseg = 1;
+            for (int q = 2; q <= want && s->ny / q >= minw; ++q)
+                if (s->ny % q == 0) s->nseg = q;
         }
     }
     const size_t smem = std::max(stream_smem(s), seam_smem(s));
@@ -448,9 +478,9 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         if (H < s->its) {
             // the newest its-H base levels carry over unchanged
             for (int q = 0; q < s->its - H; ++q)
-                PS_CUDA(s, cudaMemcpyAsync(s->base[1 - s->cur] + (size_t)q * fe,
-                                           s->base[s->cur] + (size_t)(q + H) * fe,
-                                           fe * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+                PS_CUDA(s, cudaMemcpyAsync(at(s, s->base[1 - s->cur], (size_t)q * fe),
+                                           at(s, s->base[s->cur], (size_t)(q + H) * fe),
+                                           nbytes(s, fe), cudaMemcpyDeviceToDevice, s->stream));
         }
         // algorithmic cell updates of each kernel in this half-cycle
         double cP = 0, cY = 0, cG = 0, cO = 0;
@@ -484,31 +514,39 @@ int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_
     if (!K) return fail(s, PS_ERR_UNSUPPORTED, "no standard kernel for equation %d", s->eq);
     const size_t fe = field_elems(s);
     for (int i = 0; i < 3; ++i)
-        if (!s->ring[i]) PS_CUDA(s, cudaMalloc(&s->ring[i], fe * sizeof(double)));
+        if (!s->ring[i]) PS_CUDA(s, cudaMalloc(&s->ring[i], nbytes(s, fe)));
     const int its = s->its;
     // ring[c] = current level, ring[p] = previous level
     int c = 0, p = 1, n = 2;
     double* b = s->base[s->cur];
-    PS_CUDA(s, cudaMemcpyAsync(s->ring[c], b + (size_t)(its - 1) * fe, fe * sizeof(double),
+    PS_CUDA(s, cudaMemcpyAsync(s->ring[c], at(s, b, (size_t)(its - 1) * fe), nbytes(s, fe),
                                cudaMemcpyDeviceToDevice, s->stream));
-    PS_CUDA(s, cudaMemcpyAsync(s->ring[p], b + (size_t)(its >= 2 ? its - 2 : 0) * fe,
-                               fe * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    PS_CUDA(s, cudaMemcpyAsync(s->ring[p], at(s, b, (size_t)(its >= 2 ? its - 2 : 0) * fe),
+                               nbytes(s, fe), cudaMemcpyDeviceToDevice, s->stream));
     const EqParams prm = make_params(s);
     const int every = frame_every > 0 ? frame_every : 1;
     // streaming heat kernel (64-column strips); threads = 256 keeps the generic one
     const bool fast = s->eq == PS_EQ_HEAT && s->ny % 64 == 0 && s->threads != 256;
+    const bool f32 = s->dtype == PS_DTYPE_F32;
+    if (f32 && !(fast && prm.i[0]))
+        return fail(s, PS_ERR_UNSUPPORTED,
+                    "float32 fields: heat with forward Euler and ny a multiple of 64 only");
     int rc;
     for (int64_t L = 1; L <= nlevels; ++L) {
         double* fr = nullptr;
         if (frames && L % its == 0 && (L / its) % every == 0) {
             const int64_t slot = (L / its) / every - 1;
-            if (slot < frame_cap) fr = frames + (size_t)slot * fe;
+            if (slot < frame_cap) fr = at(s, frames, (size_t)slot * fe);
         }
         const int gts = gts0 + (int)(L - 1);
         if ((rc = timed_launch(s, 4, (double)s->nx * s->ny, [&] {
                  if (fast) {
                      const dim3 grid((s->ny / 64 + 7) / 8, (s->nx + kStdRows - 1) / kStdRows);
-                     if (prm.i[0])
+                     if (f32)
+                         heat_standard_fast<false, float><<<grid, 256, 0, s->stream>>>(
+                             (const float*)s->ring[c], (const float*)s->ring[p], (float*)s->ring[n],
+                             (float*)fr, s->nx, s->ny, gts, prm.d[0]);
+                     else if (prm.i[0])
                          heat_standard_fast<false><<<grid, 256, 0, s->stream>>>(
                              s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, gts, prm.d[0]);
                      else
@@ -526,10 +564,10 @@ int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_
         n = t;
     }
     // newest levels back into the base
-    PS_CUDA(s, cudaMemcpyAsync(b + (size_t)(its - 1) * fe, s->ring[c], fe * sizeof(double),
+    PS_CUDA(s, cudaMemcpyAsync(at(s, b, (size_t)(its - 1) * fe), s->ring[c], nbytes(s, fe),
                                cudaMemcpyDeviceToDevice, s->stream));
     if (its >= 2)
-        PS_CUDA(s, cudaMemcpyAsync(b + (size_t)(its - 2) * fe, s->ring[p], fe * sizeof(double),
+        PS_CUDA(s, cudaMemcpyAsync(at(s, b, (size_t)(its - 2) * fe), s->ring[p], nbytes(s, fe),
                                    cudaMemcpyDeviceToDevice, s->stream));
     return PS_OK;
 }
@@ -592,10 +630,19 @@ int64_t ps_kernel_launches(const ps_solver* s) { return s ? s->launches : 0; }
 int ps_create(ps_solver** out, int device, int equation, int nv, int nx, int ny, int ops, int its,
               int blocksize)
 {
+    return ps_create_typed(out, device, equation, nv, nx, ny, ops, its, blocksize, PS_DTYPE_F64);
+}
+
+int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, int ny, int ops,
+                    int its, int blocksize, int dtype)
+{
     if (!out) return PS_ERR_INVALID;
     *out = nullptr;
     if (equation < PS_EQ_HEAT || equation > PS_EQ_HALF) return PS_ERR_INVALID;
+    if (dtype != PS_DTYPE_F64 && dtype != PS_DTYPE_F32) return PS_ERR_INVALID;
     ps_solver* s = new ps_solver();
+    s->dtype = dtype;
+    s->esize = dtype == PS_DTYPE_F32 ? sizeof(float) : sizeof(double);
     s->device = device;
     s->eq = equation;
     s->nv = nv;
@@ -611,6 +658,8 @@ int ps_create(ps_solver** out, int device, int equation, int nv, int nx, int ny,
     if (equation == PS_EQ_EULER && (nv != 4 || its != 2))
         rc = fail(s, PS_ERR_INVALID, "euler needs nv=4 and its=2 (got nv=%d its=%d)", nv, its);
     if (ops != s->ops) rc = fail(s, PS_ERR_INVALID, "equation %d has ops=%d, got %d", equation, s->ops, ops);
+    if (dtype == PS_DTYPE_F32 && (equation != PS_EQ_HEAT || its != 1))
+        rc = fail(s, PS_ERR_UNSUPPORTED, "float32 fields: heat with forward Euler (its=1) only");
     if (nv < 1 || nv > 4 || its < 1 || its > 2 || ops < 1 || ops > 2)
         rc = fail(s, PS_ERR_UNSUPPORTED, "nv in 1..4, its in 1..2, ops in 1..2 supported");
     if (blocksize <= 0 || blocksize % (2 * s->ops))  // io.py:52
@@ -635,7 +684,7 @@ int ps_create(ps_solver** out, int device, int equation, int nv, int nx, int ny,
         s->own_stream = true;
     }
     if (rc == PS_OK) {
-        const size_t bytes = (size_t)its * nv * nx * ny * sizeof(double);
+        const size_t bytes = nbytes(s, (size_t)its * nv * nx * ny);
         for (int i = 0; i < 2 && rc == PS_OK; ++i) {
             cudaError_t e = cudaMalloc(&s->base[i], bytes);
             if (e != cudaSuccess) rc = fail(s, PS_ERR_NOMEM, "cudaMalloc base: %s", cudaGetErrorString(e));
@@ -755,8 +804,8 @@ int ps_set_state(ps_solver* s, const double* src, int levels, int src_on_device)
     const size_t fe = field_elems(s);
     const cudaMemcpyKind kind = src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     for (int q = 0; q < s->its; ++q) {
-        const double* from = src + (size_t)(levels == 1 ? 0 : q) * fe;
-        PS_CUDA(s, cudaMemcpyAsync(s->base[s->cur] + (size_t)q * fe, from, fe * sizeof(double),
+        const double* from = at(s, const_cast<double*>(src), (size_t)(levels == 1 ? 0 : q) * fe);
+        PS_CUDA(s, cudaMemcpyAsync(at(s, s->base[s->cur], (size_t)q * fe), from, nbytes(s, fe),
                                    kind, s->stream));
     }
     if (!src_on_device) PS_CUDA(s, cudaStreamSynchronize(s->stream));
@@ -775,7 +824,7 @@ int ps_run(ps_solver* s, int mode, int64_t nlevels, int gts0, double* frames, in
     double* dframes = frames;
     const size_t fe = field_elems(s);
     if (frames && !frames_on_device) {
-        if (frame_cap > 0) PS_CUDA(s, cudaMallocAsync(&dframes, (size_t)frame_cap * fe * sizeof(double), s->stream));
+        if (frame_cap > 0) PS_CUDA(s, cudaMallocAsync(&dframes, nbytes(s, (size_t)frame_cap * fe), s->stream));
         else dframes = nullptr;
     }
     int rc;
@@ -784,7 +833,7 @@ int ps_run(ps_solver* s, int mode, int64_t nlevels, int gts0, double* frames, in
     else rc = fail(s, PS_ERR_INVALID, "mode %d", mode);
     if (frames && !frames_on_device && dframes) {
         if (rc == PS_OK)
-            PS_CUDA(s, cudaMemcpyAsync(frames, dframes, (size_t)frame_cap * fe * sizeof(double),
+            PS_CUDA(s, cudaMemcpyAsync(frames, dframes, nbytes(s, (size_t)frame_cap * fe),
                                        cudaMemcpyDeviceToHost, s->stream));
         cudaFreeAsync(dframes, s->stream);
         PS_CUDA(s, cudaStreamSynchronize(s->stream));
@@ -798,8 +847,8 @@ int ps_get_state(ps_solver* s, double* dst, int level, int dst_on_device)
     if (level < 0 || level >= s->its) return fail(s, PS_ERR_INVALID, "level %d not in [0, its)", level);
     PS_CUDA(s, cudaSetDevice(s->device));
     const size_t fe = field_elems(s);
-    PS_CUDA(s, cudaMemcpyAsync(dst, s->base[s->cur] + (size_t)(s->its - 1 - level) * fe,
-                               fe * sizeof(double),
+    PS_CUDA(s, cudaMemcpyAsync(dst, at(s, s->base[s->cur], (size_t)(s->its - 1 - level) * fe),
+                               nbytes(s, fe),
                                dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                s->stream));
     if (!dst_on_device) PS_CUDA(s, cudaStreamSynchronize(s->stream));
@@ -818,14 +867,14 @@ static int rows_copy(ps_solver* s, int level, int row0, int nrows, double* buf, 
     if (nrows == 0) return PS_OK;
     PS_CUDA(s, cudaSetDevice(s->device));
     const size_t fe = field_elems(s), plane = (size_t)s->nx * s->ny;
-    double* f = s->base[s->cur] + (size_t)(s->its - 1 - level) * fe + (size_t)row0 * s->ny;
-    const size_t width = (size_t)nrows * s->ny * sizeof(double);
+    double* f = at(s, s->base[s->cur], (size_t)(s->its - 1 - level) * fe + (size_t)row0 * s->ny);
+    const size_t width = nbytes(s, (size_t)nrows * s->ny);
     if (to_buf)
-        PS_CUDA(s, cudaMemcpy2DAsync(buf, width, f, plane * sizeof(double), width, s->nv,
+        PS_CUDA(s, cudaMemcpy2DAsync(buf, width, f, nbytes(s, plane), width, s->nv,
                                      on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                      s->stream));
     else
-        PS_CUDA(s, cudaMemcpy2DAsync(f, plane * sizeof(double), buf, width, width, s->nv,
+        PS_CUDA(s, cudaMemcpy2DAsync(f, nbytes(s, plane), buf, width, width, s->nv,
                                      on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                      s->stream));
     if (!on_device) PS_CUDA(s, cudaStreamSynchronize(s->stream));

@@ -289,15 +289,18 @@ __global__ void __launch_bounds__(NT) stream_kernel(SweptArgs a)
 // One CTA per (band, segment): the column edge at x0 = seg*wy between segment
 // seg-1 (left) and seg (right).  GAP = false: YBridge; GAP = true: the
 // Octahedron's down half.  Tile columns k <-> global x0 - KC + k, KC = OPS*(Hmax+1).
-template <class Eq, int ITS, bool GAP, int NT>
-__device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, double* sm)
+template <class Eq, int ITS, bool GAP, int NT, class T = double>
+__device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T* sm)
 {
+    const T* bin = reinterpret_cast<const T*>(a.bin);
+    const T* yface = reinterpret_cast<const T*>(a.yface);
+    T* xface = reinterpret_cast<T*>(a.xface);
     constexpr int OPS = Eq::OPS, O2 = 2 * OPS, NSLOT = ITS + 1;
     const int nv = a.nv, BX = a.bx, H = a.H, hx = a.hx, nx = a.nx, ny = a.ny;
     const int KC = OPS * (a.Hmax + 1);
     const int TW = 2 * KC;
     const int SL = nv * BX * TW;
-    double* slot = sm;
+    T* slot = sm;
     const int band = unit / a.nseg, seg = unit % a.nseg;
     const int x0 = seg_start(a, seg);
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
@@ -315,7 +318,7 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
     // level 0 (columns [KC-2OPS, KC+2OPS)) and level -1 (columns [KC-OPS, KC+OPS))
     {
         const int lo0 = GAP ? hx - O2 : 0, hi0 = GAP ? hx + O2 : BX;
-        const double* b0 = a.bin + (size_t)(ITS - 1) * nv * nx * ny;
+        const T* b0 = bin + (size_t)(ITS - 1) * nv * nx * ny;
         const int nr = hi0 - lo0, n = nv * nr * 2 * O2;
         for (int e = tid; e < n; e += NT) {
             const int k = KC - O2 + e % (2 * O2), t = e / (2 * O2);
@@ -325,8 +328,8 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
         }
         if (ITS >= 2) {
             const int lo1 = GAP ? hx - OPS : OPS, hi1 = GAP ? hx + OPS : BX - OPS;
-            const double* b1 = a.bin + (size_t)(ITS - 2) * nv * nx * ny;
-            double* s1p = slot + (NSLOT - 1) * SL;
+            const T* b1 = bin + (size_t)(ITS - 2) * nv * nx * ny;
+            T* s1p = slot + (NSLOT - 1) * SL;
             const int nr1 = hi1 - lo1, n1 = nv * nr1 * O2;
             for (int e = tid; e < n1; e += NT) {
                 const int k = KC - OPS + e % O2, t = e / O2;
@@ -341,9 +344,9 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
         const int rlo = GAP ? hx - OPS * m : OPS * m;
         const int rhi = GAP ? hx + OPS * m : BX - OPS * m;
         const int clo = KC - OPS * m, chi = KC + OPS * m;
-        double* out = slot + (m % NSLOT) * SL;
-        const double* cur = slot + ((m - 1) % NSLOT) * SL;
-        const double* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
+        T* out = slot + (m % NSLOT) * SL;
+        const T* cur = slot + ((m - 1) % NSLOT) * SL;
+        const T* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
         const int gts = a.gts_base + (int)(a.L0 + m);
         {
             const int nc = chi - clo, nr = rhi - rlo;
@@ -357,8 +360,8 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
             // y-faces of level m: left part from the left block's right edge,
             // right part from the right block's left edge.
             const int nr = rhi - rlo, n = nv * nr * O2;
-            const double* yl = a.yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
-            const double* yr = a.yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
+            const T* yl = yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
+            const T* yr = yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
             for (int e = tid; e < n; e += NT) {
                 const int j = e % O2, t = e / O2;
                 const int i = rlo + t % nr, v = t / nr;
@@ -379,7 +382,7 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
                     const int bb = rr < O2 ? bup : bdn;
                     const size_t fo =
                         ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                    out[(v * BX + i) * TW + k] = a.xface[fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny)];
+                    out[(v * BX + i) * TW + k] = xface[fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny)];
                 }
             }
         }
@@ -398,19 +401,20 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
                     const int i = side == 0 ? OPS * m + j : BX - OPS * m - O2 + j;
                     const size_t fo =
                         ((((size_t)band * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                    a.xface[fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny)] = out[(v * BX + i) * TW + k];
+                    xface[fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny)] = out[(v * BX + i) * TW + k];
                 }
             }
             const bool tob = m > H - ITS;
             const long long fs = frame_slot(a, L);
             if (tob || fs >= 0) {
                 const int nr = rhi - rlo, n = nv * nr * nc;
-                double* bo = tob ? a.bout + (size_t)(m - (H - ITS) - 1) * nv * nx * ny : nullptr;
-                double* fr = fs >= 0 ? a.frames + (size_t)fs * nv * nx * ny : nullptr;
+                T* bo = tob ? reinterpret_cast<T*>(a.bout) + (size_t)(m - (H - ITS) - 1) * nv * nx * ny
+                            : nullptr;
+                T* fr = fs >= 0 ? reinterpret_cast<T*>(a.frames) + (size_t)fs * nv * nx * ny : nullptr;
                 for (int e = tid; e < n; e += NT) {
                     const int k = clo + e % nc, t = e / nc;
                     const int i = rlo + t % nr, v = t / nr;
-                    const double val = out[(v * BX + i) * TW + k];
+                    const T val = out[(v * BX + i) * TW + k];
                     const size_t go =
                         ((size_t)v * nx + wrap(r0 + i, nx)) * ny + wrap(x0 - KC + k, ny);
                     if (bo) bo[go] = val;
@@ -421,11 +425,11 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, do
     }
 }
 
-template <class Eq, int ITS, bool GAP, int NT>
+template <class Eq, int ITS, bool GAP, int NT, class T = double>
 __global__ void __launch_bounds__(NT) seam_kernel(SweptArgs a)
 {
     extern __shared__ double sm[];
-    seam_body<Eq, ITS, GAP, NT>(a, blockIdx.x, sm);
+    seam_body<Eq, ITS, GAP, NT, T>(a, blockIdx.x, reinterpret_cast<T*>(sm));
 }
 
 }  // namespace psb

@@ -20,18 +20,35 @@ def _is_torch_cuda(x):
     return hasattr(x, "is_cuda") and hasattr(x, "data_ptr") and x.is_cuda
 
 
+def _torch_stream(device):
+    import torch
+    return torch.cuda.current_stream(device)
+
+
+DTYPES = {"float64": 0, "float32": 1}
+
+
 class Engine:
-    def __init__(self, equation, nx, ny, nv=None, ops=None, its=1, blocksize=16, device=0):
+    """dtype: "float64" (default) or "float32" (the reference's `dtype:
+    float32`: float32 fields, each level evaluated in float64 and rounded;
+    heat with forward Euler only)."""
+
+    def __init__(self, equation, nx, ny, nv=None, ops=None, its=1, blocksize=16, device=0,
+                 dtype="float64"):
         if equation not in EQ:
             raise ValueError(f"unknown equation {equation!r}; built-ins are {sorted(EQ)}")
         self.equation = equation
         self.nv = nv if nv is not None else DEFAULT_NV.get(equation, 1)
         self.ops = ops if ops is not None else DEFAULT_OPS.get(equation, 1)
         self.nx, self.ny, self.its, self.bs, self.device = nx, ny, its, blocksize, device
+        self.dtype = np.dtype(dtype)
+        if self.dtype.name not in DTYPES:
+            raise ValueError(f"dtype {dtype!r}: float64 or float32")
         self._h = ctypes.c_void_p()
+        self._stream = None  # cudaStream_t set by set_stream (None: the solver's own)
         L = _lib.lib()
-        rc = L.ps_create(ctypes.byref(self._h), device, EQ[equation], self.nv, nx, ny, self.ops,
-                         its, blocksize)
+        rc = L.ps_create_typed(ctypes.byref(self._h), device, EQ[equation], self.nv, nx, ny,
+                               self.ops, its, blocksize, DTYPES[self.dtype.name])
         _lib.check(rc, None)
         self.shape = (self.nv, nx, ny)
 
@@ -67,24 +84,44 @@ class Engine:
         check(_lib.lib().ps_configure(self._h, h, nseg, chunk, threads), self._h)
 
     # -- state -------------------------------------------------------------
+    # Torch tensors are read and written on the solver's stream.  Unless that
+    # stream is torch's current one, the solver first waits for work queued on
+    # torch's stream (the tensor's producer) and, after writing into a
+    # tensor, waits for its own copy before returning.
+    def _shared_stream(self):
+        return self._stream is not None and self._stream == _torch_stream(self.device).cuda_stream
+
+    def _before_read(self):
+        if not self._shared_stream():
+            _torch_stream(self.device).synchronize()
+
+    def _after_write(self):
+        if not self._shared_stream():
+            self.synchronize()
+
     def set_state(self, field):
         """Initial levels: one field (copied to every base level) or `its` fields."""
         if _is_torch_cuda(field):
+            self._before_read()
             levels = field.numel() // (self.nv * self.nx * self.ny)
             check(_lib.lib().ps_set_state(self._h, ctypes.c_void_p(field.data_ptr()), levels, 1),
                   self._h)
+            self._after_write()  # the tensor may be released once this returns
             return
-        a = np.ascontiguousarray(field, dtype=np.float64)
+        a = np.ascontiguousarray(field, dtype=self.dtype)
         levels = a.size // (self.nv * self.nx * self.ny)
         check(_lib.lib().ps_set_state(self._h, a.ctypes.data_as(ctypes.c_void_p), levels, 0),
               self._h)
 
     def get_state(self, level=0, out=None):
         if out is not None and _is_torch_cuda(out):
+            self._before_read()
             check(_lib.lib().ps_get_state(self._h, ctypes.c_void_p(out.data_ptr()), level, 1),
                   self._h)
+            self._after_write()
             return out
-        a = out if out is not None else np.empty(self.shape)
+        a = out if out is not None else np.empty(self.shape, dtype=self.dtype)
+        assert a.dtype == self.dtype and a.flags.c_contiguous
         check(_lib.lib().ps_get_state(self._h, a.ctypes.data_as(ctypes.c_void_p), level, 0),
               self._h)
         return a
@@ -93,10 +130,12 @@ class Engine:
         """Rows [row0, row0+nrows) of base level `level` (0 = newest) as a
         (nv, nrows, ny) array, or into `out` (numpy or torch CUDA)."""
         if out is not None and _is_torch_cuda(out):
+            self._before_read()
             check(_lib.lib().ps_get_rows(self._h, level, row0, nrows,
                                          ctypes.c_void_p(out.data_ptr()), 1), self._h)
+            self._after_write()
             return out
-        a = out if out is not None else np.empty((self.nv, nrows, self.ny))
+        a = out if out is not None else np.empty((self.nv, nrows, self.ny), dtype=self.dtype)
         check(_lib.lib().ps_get_rows(self._h, level, row0, nrows,
                                      a.ctypes.data_as(ctypes.c_void_p), 0), self._h)
         return a
@@ -105,18 +144,22 @@ class Engine:
         """Overwrite rows [row0, row0+k) of base level `level` from a
         (nv, k, ny) array (numpy or torch CUDA)."""
         if _is_torch_cuda(rows):
+            self._before_read()
             k = rows.numel() // (self.nv * self.ny)
             check(_lib.lib().ps_set_rows(self._h, level, row0, k,
                                          ctypes.c_void_p(rows.data_ptr()), 1), self._h)
+            self._after_write()
             return
-        a = np.ascontiguousarray(rows, dtype=np.float64)
+        a = np.ascontiguousarray(rows, dtype=self.dtype)
         k = a.size // (self.nv * self.ny)
         check(_lib.lib().ps_set_rows(self._h, level, row0, k, a.ctypes.data_as(ctypes.c_void_p), 0),
               self._h)
 
     def run(self, nlevels, mode="swept", gts0=1, frames=None, frame_every=1):
         """Advance `nlevels` levels.  frames: None, a host array or a device tensor of
-        shape (k, nv, nx, ny) receiving every `frame_every`-th full step."""
+        shape (k, nv, nx, ny) receiving every `frame_every`-th full step.  The
+        run is queued on the solver's stream; device frames are complete after
+        synchronize() (or at once for work queued later on the same stream)."""
         if frames is None:
             rc = _lib.lib().ps_run(self._h, MODE[mode], int(nlevels), gts0, None, 0, frame_every, 0)
         elif _is_torch_cuda(frames):
@@ -124,7 +167,7 @@ class Engine:
                                    ctypes.c_void_p(frames.data_ptr()), frames.shape[0],
                                    frame_every, 1)
         else:
-            assert frames.dtype == np.float64 and frames.flags.c_contiguous
+            assert frames.dtype == self.dtype and frames.flags.c_contiguous
             rc = _lib.lib().ps_run(self._h, MODE[mode], int(nlevels), gts0,
                                    frames.ctypes.data_as(ctypes.c_void_p), frames.shape[0],
                                    frame_every, 0)
@@ -151,6 +194,7 @@ class Engine:
 
     def set_stream(self, stream_handle):
         check(_lib.lib().ps_set_stream(self._h, ctypes.c_void_p(stream_handle)), self._h)
+        self._stream = stream_handle or None
 
     @property
     def launches(self):

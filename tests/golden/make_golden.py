@@ -156,12 +156,12 @@ class _Capture:
         # attribute is enough.
 
 
-def run_reference(pysweep, cap, eqn, ic, globals_, bs, ops, its, swept):
+def run_reference(pysweep, cap, eqn, ic, globals_, bs, ops, its, swept, dtype="float64"):
     eqdir = os.path.join(os.path.dirname(pysweep.__file__), "equations")
     cap.frames = []
     solver = pysweep.Solver(ic, None, sendWarning=False)
-    solver.dtypeStr = "float64"
-    solver.dtype = np.dtype("float64")
+    solver.dtypeStr = dtype
+    solver.dtype = np.dtype(dtype)
     solver.verbose = False
     solver.share = 0
     solver.simulation = swept
@@ -228,6 +228,13 @@ CASES = [
     ("half_n24_bs8", "half", 24, 8, 1, 2, "half", 10),
 ]
 
+# FP32 runs of the reference (yaml `dtype: float32`, io.py:72-73): the shared
+# array and the frames are float32; the initial field is rounded to float32.
+CASES_F32 = [
+    ("heat_fe_f32_n64_bs16", "heat", 64, 16, 1, 1, "heat_fe", 37),
+    ("heat_fe_f32_n128_bs32", "heat", 128, 32, 1, 1, "heat_fe", 45),
+]
+
 
 def make_globals(kind, n, steps):
     if kind in ("heat_fe", "heat_rk2"):
@@ -250,6 +257,21 @@ def make_globals(kind, n, steps):
 def main(refroot):
     pysweep, io, solver_mod = _import_reference(refroot)
     cap = _Capture(io, solver_mod)
+    for name, eqn, n, bs, ops, its, gkind, steps in CASES_F32:
+        ic = heat_ic(n).astype(np.float32).astype(np.float64)
+        g = make_globals(gkind, n, steps)
+        out = {}
+        for swept in (True, False):
+            frames, nframes_ref = run_reference(pysweep, cap, eqn, ic, g, bs, ops, its, swept,
+                                                dtype="float32")
+            key = "swept" if swept else "standard"
+            out[key] = frames
+            out[key + "_array_shape0"] = np.int64(nframes_ref)
+            print(f"{name:24s} {key:8s} frames={frames.shape[0]}", flush=True)
+        np.savez_compressed(
+            os.path.join(HERE, name + ".npz"),
+            eqn=eqn, n=n, bs=bs, ops=ops, its=its, globals=np.array(g, dtype=np.float64),
+            ic=ic, dtype="float32", **out)
     for name, eqn, n, bs, ops, its, gkind, steps in CASES:
         if eqn == "heat":
             ic = heat_ic(n)
