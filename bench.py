@@ -468,6 +468,8 @@ def run_euler(args):
     eng = Engine("euler", n, n, its=2, blocksize=bs)
     for k, v in plugin_constants("euler", g).items():
         eng.set_global(k, v)
+    if args.euler_chunk:
+        eng.configure(chunk=args.euler_chunk)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
@@ -499,7 +501,8 @@ def run_euler(args):
             "standard": cells / (ms_st / 1000) / 1e9, "swept_ms": ms_sw, "standard_ms": ms_st,
             "swept_equals_standard": bool(np.array_equal(out_sw, out_st)),
             "kernel_share": {k: v / sum(kinds.values()) for k, v in kinds.items()},
-            "n": n, "time_steps": steps, "blocksize": bs, "stages_per_step": 2,
+            "n": n, "time_steps": steps, "blocksize": bs, "chunk": args.euler_chunk or "default",
+            "stages_per_step": 2,
             "dtype": "f64", "data": "synthetic", "steps": args.steps}
     print(json.dumps(line), flush=True)
     eng.close()
@@ -728,7 +731,8 @@ def main():
                     help="Euler swept vs standard (separate JSON line)")
     ap.add_argument("--euler-n", type=int, default=4096)
     ap.add_argument("--euler-steps", type=int, default=1000)
-    ap.add_argument("--euler-bs", type=int, default=32)
+    ap.add_argument("--euler-bs", type=int, default=16)
+    ap.add_argument("--euler-chunk", type=int, default=0, help="32 or 64 (0: the default)")
     ap.add_argument("--adjoint", action="store_true",
                     help="inverse heat problem: adjoint vs forward cost (separate JSON line)")
     ap.add_argument("--adj-n", type=int, default=2048)

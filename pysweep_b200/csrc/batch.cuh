@@ -37,8 +37,12 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3)
     heat_fast_body<BX, GAP>(a, u.y, sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
+// The generic batched kernels hold the descriptor fields in registers (the
+// single-instance kernels read them from the parameter bank), so they are
+// capped at the single-instance register budget to keep two stream CTAs (four
+// seam CTAs) per SM.
 template <class Eq, int ITS, int W, bool GAP, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 2)
     stream_batch(const SweptArgs* __restrict__ desc, const int2* __restrict__ units, int parity,
                  int H, long long L0)
 {
@@ -50,7 +54,7 @@ __global__ void __launch_bounds__(NT)
 }
 
 template <class Eq, int ITS, bool GAP, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
     seam_batch(const SweptArgs* __restrict__ desc, const int2* __restrict__ units, int parity,
                int H, long long L0)
 {

@@ -247,6 +247,7 @@ bool pick_swept(int eq, int ops, int its, int chunk, SweptSet* out)
     PS_SET(PS_EQ_HEAT, 1, 1, 64, Heat)
     PS_SET(PS_EQ_HEAT, 1, 2, 64, Heat)
     PS_SET(PS_EQ_EULER, 2, 2, 32, Euler)
+    PS_SET(PS_EQ_EULER, 2, 2, 64, Euler)
     PS_SET(PS_EQ_HALF, 1, 1, 32, Half)
     PS_SET(PS_EQ_HALF, 1, 2, 32, Half)
     PS_SET(PS_EQ_EXAMPLE, 1, 1, 32, ExampleT<1>)
@@ -673,6 +674,12 @@ int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, i
         rc = fail(s, PS_ERR_INVALID, "blocksize %d gives no swept level (MPSS < 1)", blocksize);
     s->H = s->mpss;
     s->chunk = (2 * s->ops * (s->H + 1) <= 32) ? 32 : 64;
+    // Euler: 64-column chunks keep every thread of a stream CTA busy on each
+    // level, where the tile fits in shared memory
+    if (s->eq == PS_EQ_EULER && s->chunk == 32) {
+        s->chunk = 64;
+        if (stream_smem(s) > 227 * 1024) s->chunk = 32;
+    }
     s->nseg = 1;
     if (rc == PS_OK) {
         cudaError_t e = cudaSetDevice(device);
@@ -959,6 +966,7 @@ struct BatchInst {
 
 struct ps_batch {
     int device = 0, eq = 0, nv = 1, ops = 1, its = 1, bs = 0, mpss = 0, H = 0;
+    int chunk = 32;  // column chunk of the generic streams (32 or 64)
     bool fast = false;
     cudaStream_t stream = nullptr;
     std::vector<BatchInst> inst;
@@ -1038,7 +1046,7 @@ int batch_upload(ps_batch* b)
             a.nb = I.nb;
             a.nseg = I.nseg;
             a.wy = I.ny / I.nseg;
-            a.nchunks = b->fast ? a.wy / kFastChunk : (a.wy + 31) / 32;
+            a.nchunks = b->fast ? a.wy / kFastChunk : (a.wy + b->chunk - 1) / b->chunk;
             a.seg_unit = b->fast ? 32 : a.wy;
             a.seg_units = b->fast ? I.ny / 32 : I.nseg;
             a.off = par ? b->bs / 2 : 0;  // prism bands alternate by half a block
@@ -1057,7 +1065,7 @@ int batch_upload(ps_batch* b)
 size_t batch_stream_smem(const ps_batch* b)
 {
     if (b->fast) return b->bs == 16 ? heat_fast_smem<16>(b->H) : heat_fast_smem<32>(b->H);
-    const int O2 = 2 * b->ops, RS = 32 + O2;
+    const int O2 = 2 * b->ops, RS = b->chunk + O2;
     return sizeof(double) * ((size_t)(b->its + 1) * b->nv * b->bs * RS +
                              (size_t)(b->H + 1) * b->nv * b->bs * O2);
 }
@@ -1078,7 +1086,7 @@ struct BatchKernels {
 };
 
 // Enqueue one half-cycle for every instance.
-template <class Eq, int ITS>
+template <class Eq, int ITS, int W>
 void batch_half(ps_batch* b, int par, int H, long long L0, size_t ssm, size_t gsm, dim3 fgrid)
 {
     const int nu = b->nunits;
@@ -1095,22 +1103,22 @@ void batch_half(ps_batch* b, int par, int H, long long L0, size_t ssm, size_t gs
             seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
         }
     } else {
-        stream_batch<Eq, ITS, 32, false, 256><<<nu, 256, gsm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+        stream_batch<Eq, ITS, W, false, 256><<<nu, 256, gsm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
         seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
-        stream_batch<Eq, ITS, 32, true, 256><<<nu, 256, gsm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+        stream_batch<Eq, ITS, W, true, 256><<<nu, 256, gsm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
         seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
     }
 }
 
-template <class Eq, int ITS>
+template <class Eq, int ITS, int W>
 void batch_prepare()
 {
     allow_big_smem(heat_stream_fast_batch<16, false>);
     allow_big_smem(heat_stream_fast_batch<16, true>);
     allow_big_smem(heat_stream_fast_batch<32, false>);
     allow_big_smem(heat_stream_fast_batch<32, true>);
-    allow_big_smem(stream_batch<Eq, ITS, 32, false, 256>);
-    allow_big_smem(stream_batch<Eq, ITS, 32, true, 256>);
+    allow_big_smem(stream_batch<Eq, ITS, W, false, 256>);
+    allow_big_smem(stream_batch<Eq, ITS, W, true, 256>);
     allow_big_smem(seam_batch<Eq, ITS, false, 128>);
     allow_big_smem(seam_batch<Eq, ITS, true, 128>);
 }
@@ -1118,18 +1126,19 @@ void batch_prepare()
 using HalfFn = void (*)(ps_batch*, int, int, long long, size_t, size_t, dim3);
 using PrepFn = void (*)();
 
-bool batch_pick(int eq, int ops, int its, HalfFn* half, PrepFn* prep)
+bool batch_pick(int eq, int ops, int its, int chunk, HalfFn* half, PrepFn* prep)
 {
-#define PS_BSET(EQ, OP, IT, T)                          \
-    if (eq == EQ && ops == OP && its == IT) {           \
-        *half = batch_half<T, IT>;                      \
-        *prep = batch_prepare<T, IT>;                   \
-        return true;                                    \
+#define PS_BSET(EQ, OP, IT, W, T)                                   \
+    if (eq == EQ && ops == OP && its == IT && chunk == W) {         \
+        *half = batch_half<T, IT, W>;                               \
+        *prep = batch_prepare<T, IT, W>;                            \
+        return true;                                                \
     }
-    PS_BSET(PS_EQ_HEAT, 1, 1, Heat)
-    PS_BSET(PS_EQ_HEAT, 1, 2, Heat)
-    PS_BSET(PS_EQ_EULER, 2, 2, Euler)
-    PS_BSET(PS_EQ_HALF, 1, 2, Half)
+    PS_BSET(PS_EQ_HEAT, 1, 1, 32, Heat)
+    PS_BSET(PS_EQ_HEAT, 1, 2, 32, Heat)
+    PS_BSET(PS_EQ_EULER, 2, 2, 32, Euler)
+    PS_BSET(PS_EQ_EULER, 2, 2, 64, Euler)
+    PS_BSET(PS_EQ_HALF, 1, 2, 32, Half)
 #undef PS_BSET
     return false;
 }
@@ -1177,7 +1186,7 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
     *out = nullptr;
     HalfFn half;
     PrepFn prep;
-    if (!batch_pick(equation, ops, its, &half, &prep))
+    if (!batch_pick(equation, ops, its, 32, &half, &prep))
         return bfail(nullptr, PS_ERR_UNSUPPORTED, "no batched kernels for equation %d ops %d its %d",
                      equation, ops, its);
     if (equation == PS_EQ_EULER && nv != 4) return bfail(nullptr, PS_ERR_INVALID, "euler needs nv=4");
@@ -1195,6 +1204,11 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
     b->mpss = blocksize / (2 * ops) - 1;
     b->H = b->mpss;
     b->fast = equation == PS_EQ_HEAT && its == 1 && (blocksize == 16 || blocksize == 32);
+    // Euler: 64-column chunks where the tile fits (as for a single solver)
+    if (!b->fast && equation == PS_EQ_EULER) {
+        b->chunk = 64;
+        if (batch_stream_smem(b) > 227 * 1024) b->chunk = 32;
+    }
     int rc = PS_OK;
     std::vector<int2> units;
     for (int i = 0; i < count && rc == PS_OK; ++i) {
@@ -1209,8 +1223,17 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
         else if (!b->fast && 32 < 2 * ops * (b->H + 1))
             rc = bfail(b, PS_ERR_UNSUPPORTED, "blocksize %d too large for the batched streams", blocksize);
         I.nb = I.nx / blocksize;
-        // register streams: segments of about four 64-column chunks
-        I.nseg = b->fast ? std::max(1, I.ny / (4 * kFastChunk)) : 1;
+        // segments of about 256 columns, so that the units of large and small
+        // instances take similar times (a phase waits for its slowest unit);
+        // the generic streams need segments that divide ny and hold a chunk
+        if (b->fast) {
+            I.nseg = std::max(1, I.ny / (4 * kFastChunk));
+        } else {
+            const int minw = std::max(b->chunk, 2 * ops * (b->H + 1));
+            I.nseg = 1;
+            for (int q = 2; q <= I.ny / 256 && I.ny / q >= minw; ++q)
+                if (I.ny % q == 0) I.nseg = q;
+        }
         for (int u = 0; u < I.nb * I.nseg; ++u) units.push_back(make_int2(i, u));
         b->inst.push_back(I);
     }
@@ -1239,6 +1262,9 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
             e = cudaMemcpy(b->d_units, units.data(), units.size() * sizeof(int2), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) rc = bfail(b, PS_ERR_NOMEM, "batch tables: %s", cudaGetErrorString(e));
     }
+    // the kernels of the chosen chunk width (prep opts them into large shared memory)
+    if (rc == PS_OK && !batch_pick(equation, ops, its, b->chunk, &half, &prep))
+        rc = bfail(b, PS_ERR_UNSUPPORTED, "no batched kernels for chunk %d", b->chunk);
     if (rc == PS_OK) prep();
     if (rc != PS_OK) {
         g_create_error = b->err;
@@ -1308,7 +1334,7 @@ int ps_batch_run(ps_batch* b, int64_t nlevels, int use_graph)
     PSB_CUDA(b, cudaSetDevice(b->device));
     HalfFn half;
     PrepFn prep;
-    batch_pick(b->eq, b->ops, b->its, &half, &prep);
+    batch_pick(b->eq, b->ops, b->its, b->chunk, &half, &prep);
     const int64_t nhalf = (nlevels + b->H - 1) / b->H;
     if (!use_graph) {
         int rc = batch_upload(b);

@@ -78,6 +78,7 @@ CONFIGS = [
     ("euler", 64, 16, 2, 2, 12, None, {}),
     ("euler", 64, 32, 2, 2, 10, None, {"nseg": 2}),
     ("euler", 96, 16, 2, 2, 9, None, {"h": 2, "nseg": 3}),
+    ("euler", 128, 16, 2, 2, 9, None, {"chunk": 64}),
     ("half", 64, 16, 1, 2, 20, None, {}),
     ("checker", 48, 8, 2, 2, 12, False, {}),
     ("example", 48, 12, 1, 1, 21, True, {"nseg": 2}),
