@@ -7,6 +7,7 @@ vortex of euler.py:63-116.
 import numpy
 
 from pysweep_b200.solver import driver_shim as cuda
+from pysweep_b200.solver import write_field
 
 gamma = 1.4
 
@@ -46,3 +47,19 @@ def analytical_array(npx, npy, t, **kw):
     y = numpy.linspace(-5, 5, npy, endpoint=False)
     X, Y = numpy.meshgrid(x, y, indexing="ij")
     return vortex(X, Y, t, **kw)
+
+
+def analytical(x, y, t, gamma=1.4, alpha=numpy.pi / 4):
+    """The vortex of pysweep/equations/euler.py:63-116 (strength 5)."""
+    return vortex(x, y, t, gamma=gamma, alpha=alpha)
+
+
+def createInitialConditions(npx, npy, t=0, gamma=1.4, filename="eulerConditions.hdf5"):
+    """The initial field file of pysweep/equations/euler.py:33-56: dataset
+    "data" of shape (4, npx, npy) on linspace(-5, 5, n, endpoint=True).  HDF5
+    through h5py when it is importable, else an .npz next to `filename`;
+    returns the path written."""
+    X = numpy.linspace(-5, 5, npx, endpoint=True)
+    Y = numpy.linspace(-5, 5, npy, endpoint=True)
+    Xg, Yg = numpy.meshgrid(X, Y, indexing="ij")
+    return write_field(analytical(Xg, Yg, t, gamma=gamma), filename)

@@ -7,6 +7,7 @@ sine of heat.py:95-113.
 import numpy
 
 from pysweep_b200.solver import driver_shim as cuda
+from pysweep_b200.solver import write_field
 
 scheme = True
 
@@ -29,3 +30,21 @@ def analytical(npx, npy, t, alpha=0.1):
     Y = numpy.linspace(0, 1, npy, endpoint=False)
     u = numpy.sin(2 * numpy.pi * X)[:, None] * numpy.sin(2 * numpy.pi * Y)[None, :]
     return (u * numpy.exp(-8 * numpy.pi ** 2 * alpha * t))[None], X, Y
+
+
+def analyticalEquation(x, y, t, alpha=0.1):
+    """sin(2 pi x) sin(2 pi y) exp(-8 pi^2 alpha t) (pysweep/equations/heat.py:90-93)."""
+    m = n = 2
+    return (numpy.sin(m * numpy.pi * x) * numpy.sin(n * numpy.pi * y) *
+            numpy.exp(-(m * m + n * n) * numpy.pi * numpy.pi * alpha * t))
+
+
+def createInitialConditions(npx, npy, alpha=0.1, t=0, filename="heatConditions.hdf5"):
+    """The initial field file of pysweep/equations/heat.py:66-88: dataset
+    "data" of shape (1, npx, npy) on linspace(0, 1, n, endpoint=True).  HDF5
+    through h5py when it is importable, else an .npz next to `filename`;
+    returns the path written."""
+    X = numpy.linspace(0, 1, npx, endpoint=True)
+    Y = numpy.linspace(0, 1, npy, endpoint=True)
+    data = analyticalEquation(X[:, None], Y[None, :], t, alpha=alpha)[None]
+    return write_field(data, filename)

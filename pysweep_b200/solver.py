@@ -293,6 +293,23 @@ class Solver:
               f"{getattr(self, 'timeSteps', None)}, {moment}")
 
 
+def write_field(data, filename):
+    """Write an initial field as dataset "data": HDF5 when h5py is importable,
+    otherwise an .npz with the same dataset name next to `filename`.  Returns
+    the path written (readable by Solver(initialConditions=path))."""
+    try:
+        import h5py
+    except ImportError:
+        h5py = None
+    if h5py is not None:
+        with h5py.File(filename, "w") as f:
+            f.create_dataset("data", data=data)
+        return filename
+    base, _ = os.path.splitext(filename)
+    np.savez(base + ".npz", data=data)
+    return base + ".npz"
+
+
 def _read_data(path):
     if path.endswith(".npy"):
         return np.load(path)

@@ -7,6 +7,8 @@ import numpy as np
 import pytest
 import yaml
 
+import oracle
+
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 EQDIR = os.path.join(os.path.dirname(HERE), "pysweep_b200", "equations")
@@ -44,3 +46,20 @@ def test_solver_yaml_matches_reference_frames(tmp_path, name, swept):
     out = glob.glob(str(tmp_path / "out.*"))
     assert out, "no output file written"
     assert (tmp_path / "log.yaml").exists()
+
+
+def test_command_line_heat_runs_swept_and_standard(tmp_path, monkeypatch):
+    """python -m pysweep_b200 -f heat [--swept] -b 8 -nx 32 -nt 12: the two
+    decompositions give the same frames, equal to the oracle's."""
+    from pysweep_b200 import commandline
+    monkeypatch.chdir(tmp_path)
+    runs = {}
+    for swept in (True, False):
+        argv = ["-f", "heat", "-b", "8", "-nx", "32", "-nt", "12", "--ignore"]
+        s = commandline.main(argv + (["--swept"] if swept else []))
+        runs[swept] = s.data
+    assert np.array_equal(runs[True][-1], runs[False][-1])
+    ic = s.initialConditions
+    nlev = len(runs[False]) - 1
+    _, want, _ = oracle.standard("heat", ic, s.globals, 1, nlev, frames=False)
+    assert np.array_equal(runs[False][-1], want)
