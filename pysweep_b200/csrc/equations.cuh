@@ -239,11 +239,123 @@ __device__ __forceinline__ void dflux(double gamma, double gm1, const double* __
     }
 }
 
+// One face between cells a (lower index) and b = a+1 in direction DIR: its
+// flux f and spectral term s from q at a and b and the pressures at a-1, a,
+// b, b+1.  dflux evaluates exactly this (same operations, same arguments)
+// twice for every face, as the upper face of cell a and the lower face of
+// cell b; the face-sharing kernels evaluate it once.
+template <int DIR>
+__device__ __forceinline__ void face(double gamma, double gm1, const double* qa, const double* qb,
+                                     double Pam, double Pa, double Pb, double Pbp, double* f,
+                                     double* s)
+{
+    double L[4], R[4];
+    const double dab = __dsub_rn(Pb, Pa);
+    limiter(qa, qb, dab, __dsub_rn(Pa, Pam), L);
+    limiter(qb, qa, dab, __dsub_rn(Pbp, Pb), R);
+    flux<DIR>(gm1, L, R, f);
+    spectral<DIR>(gamma, gm1, L, R, s);
+}
+
+// A cell's derivative term from its lower (lo) and upper (hi) faces, each
+// [flux 0..3, spectral 4..7], in dflux's order.
+__device__ __forceinline__ double dface(const double* lo, const double* hi, int v)
+{
+    return __dmul_rn(__dsub_rn(__dsub_rn(__dadd_rn(__dadd_rn(0.0, lo[v]), lo[4 + v]), hi[v]),
+                               hi[4 + v]),
+                     0.5);
+}
+
+// The stage update of Euler::step (euler.py:131-156)
+__device__ __forceinline__ double update(double u, double up, double fx, double fy, double dtdx,
+                                         double dtdy, bool full)
+{
+    const double d = __dadd_rn(__dmul_rn(fx, dtdx), __dmul_rn(fy, dtdy));
+    return full ? __dadd_rn(up, d) : __dadd_rn(u, __dmul_rn(0.5, d));
+}
+
 }  // namespace euler
+
+// Scratch of Euler::level for a tile of bx rows and chunk w (doubles):
+// pressures [bx][w+4], faces [(bx-3)*(w+1)][8], x-direction terms [(bx-4)*w][4].
+__host__ __device__ constexpr int euler_level_scratch(int bx, int w)
+{
+    return bx * (w + 4) + 8 * (bx - 3) * (w + 1) + 4 * (bx - 4) * w;
+}
 
 struct Euler {
     static constexpr int OPS = 2;
     static constexpr int ID = EQ_EULER;
+    static constexpr bool kFaceLevel = true;  // stream tiles use level() below
+
+    // One level of a stream tile with faces shared between cells: out[i][kc+2]
+    // from cur around (i, kc) and prv[i][kc-2] (the offsets of Eq::step in
+    // stream_body) for rows [rlo, rhi) and columns kc in [kc0, kc1) of
+    // [4][bx][rs] tiles.  Every thread of the CTA calls it (it synchronises);
+    // scratch holds euler_level_scratch(bx, rs - 4) doubles.
+    template <int NT>
+    __device__ static void level(const double* __restrict__ cur, const double* __restrict__ prv,
+                                 double* __restrict__ out, int rlo, int rhi, int kc0, int kc1,
+                                 int rs, int bx, int gts, const EqParams& p, double* scratch,
+                                 int tid)
+    {
+        const int vs = bx * rs;
+        const int nr = rhi - rlo, nc = kc1 - kc0;
+        if (nr <= 0 || nc <= 0) return;  // the same for every thread
+        const double dtdx = p.d[0], dtdy = p.d[1], gamma = p.d[2], gm1 = p.d[3];
+        double* P = scratch;                      // [bx][rs]
+        double* F = P + bx * rs;                  // faces, [.][8]
+        double* D = F + 8 * (bx - 3) * (rs - 3);  // x terms, [nr][nc][4]
+        const int pc = nc + 4, npr = (nr + 4) * pc;
+        for (int e = tid; e < npr; e += NT) {
+            const int o = (rlo - 2 + e / pc) * rs + kc0 - 2 + e % pc;
+            P[o] = euler::pressure(gm1, cur[o], cur[o + vs], cur[o + 2 * vs], cur[o + 3 * vs]);
+        }
+        __syncthreads();
+        // faces between rows rlo-1+j and rlo+j
+        for (int e = tid; e < (nr + 1) * nc; e += NT) {
+            const int a = (rlo - 1 + e / nc) * rs + kc0 + e % nc, b = a + rs;
+            double qa[4], qb[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                qa[v] = cur[a + v * vs];
+                qb[v] = cur[b + v * vs];
+            }
+            euler::face<1>(gamma, gm1, qa, qb, P[a - rs], P[a], P[b], P[b + rs], F + e * 8,
+                           F + e * 8 + 4);
+        }
+        __syncthreads();
+        for (int e = tid; e < nr * nc; e += NT) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) D[e * 4 + v] = euler::dface(F + e * 8, F + (e + nc) * 8, v);
+        }
+        __syncthreads();
+        // faces between columns kc0-1+c and kc0+c
+        for (int e = tid; e < nr * (nc + 1); e += NT) {
+            const int a = (rlo + e / (nc + 1)) * rs + kc0 - 1 + e % (nc + 1), b = a + 1;
+            double qa[4], qb[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                qa[v] = cur[a + v * vs];
+                qb[v] = cur[b + v * vs];
+            }
+            euler::face<2>(gamma, gm1, qa, qb, P[a - 1], P[a], P[b], P[b + 1], F + e * 8,
+                           F + e * 8 + 4);
+        }
+        __syncthreads();
+        const bool full = gts % 2 == 0;
+        for (int e = tid; e < nr * nc; e += NT) {
+            const int i = e / nc, c = e % nc;
+            const int o = (rlo + i) * rs + kc0 + c;
+            const double* lo = F + (i * (nc + 1) + c) * 8;
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                out[o + OPS + v * vs] =
+                    euler::update(cur[o + v * vs], prv[o - OPS + v * vs], D[e * 4 + v],
+                                  euler::dface(lo, lo + 8, v), dtdx, dtdy, full);
+        }
+    }
+
     __device__ static __forceinline__ void step(const double* __restrict__ u,
                                                 const double* __restrict__ up,
                                                 double* __restrict__ o, const Nbr& n, int gts,
@@ -266,6 +378,12 @@ struct Euler {
                     __dmul_rn(0.5, __dadd_rn(__dmul_rn(fx[v], dtdx), __dmul_rn(fy[v], dtdy))));
         }
     }
+};
+
+// Euler with the per-cell step in the stream tiles too (blocksizes whose
+// tile leaves no room for the face scratch)
+struct EulerCell : Euler {
+    static constexpr bool kFaceLevel = false;
 };
 
 }  // namespace psb

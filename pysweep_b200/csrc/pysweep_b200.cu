@@ -15,6 +15,7 @@
 #include "swept.cuh"
 #include "heat_fast.cuh"
 #include "standard_fast.cuh"
+#include "euler_faces.cuh"
 #include "batch.cuh"
 
 namespace psb {
@@ -238,6 +239,10 @@ SweptSet make_set()
 }
 
 // (equation, ops, its, chunk) -> kernels; nullptr members = not built.
+// Euler's stream tiles with the per-cell step (see EulerCell): an internal
+// equation id for kernel selection only
+constexpr int PS_EQ_EULER_CELL = 100;
+
 bool pick_swept(int eq, int ops, int its, int chunk, SweptSet* out)
 {
 #define PS_SET(EQ, OP, IT, W, T) \
@@ -248,6 +253,8 @@ bool pick_swept(int eq, int ops, int its, int chunk, SweptSet* out)
     PS_SET(PS_EQ_HEAT, 1, 2, 64, Heat)
     PS_SET(PS_EQ_EULER, 2, 2, 32, Euler)
     PS_SET(PS_EQ_EULER, 2, 2, 64, Euler)
+    PS_SET(PS_EQ_EULER_CELL, 2, 2, 32, EulerCell)
+    PS_SET(PS_EQ_EULER_CELL, 2, 2, 64, EulerCell)
     PS_SET(PS_EQ_HALF, 1, 1, 32, Half)
     PS_SET(PS_EQ_HALF, 1, 2, 32, Half)
     PS_SET(PS_EQ_EXAMPLE, 1, 1, 32, ExampleT<1>)
@@ -354,11 +361,28 @@ int ensure_swept_buffers(ps_solver* s)
     return PS_OK;
 }
 
-size_t stream_smem(const ps_solver* s)
+size_t stream_tile_smem(const ps_solver* s)
 {
     const int O2 = 2 * s->ops, RS = s->chunk + O2;
     return s->esize * ((size_t)(s->its + 1) * s->nv * s->bs * RS +
                        (size_t)(s->H + 1) * s->nv * s->bs * O2);
+}
+
+// Euler streams share faces between cells when tile and scratch still leave
+// room for two CTAs per SM (measured: with one CTA per SM the per-cell step
+// on a wider chunk is faster; Euler stream levels are latency-bound)
+constexpr size_t kFaceSmemCap = 113 * 1024;
+bool euler_faces_fit(const ps_solver* s)
+{
+    return s->eq == PS_EQ_EULER &&
+           stream_tile_smem(s) + sizeof(double) * euler_level_scratch(s->bs, s->chunk) <=
+               kFaceSmemCap;
+}
+
+size_t stream_smem(const ps_solver* s)
+{
+    return stream_tile_smem(s) +
+           (euler_faces_fit(s) ? sizeof(double) * euler_level_scratch(s->bs, s->chunk) : 0);
 }
 
 size_t seam_smem(const ps_solver* s)
@@ -371,7 +395,8 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
               int frame_every)
 {
     SweptSet K;
-    if (!pick_swept(s->eq, s->ops, s->its, s->chunk, &K))
+    const int keq = (s->eq == PS_EQ_EULER && !euler_faces_fit(s)) ? PS_EQ_EULER_CELL : s->eq;
+    if (!pick_swept(keq, s->ops, s->its, s->chunk, &K))
         return fail(s, PS_ERR_UNSUPPORTED, "no swept kernels for equation %d ops %d its %d chunk %d",
                     s->eq, s->ops, s->its, s->chunk);
     const int O2 = 2 * s->ops;
@@ -529,6 +554,9 @@ int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_
     // streaming heat kernel (64-column strips); threads = 256 keeps the generic one
     const bool fast = s->eq == PS_EQ_HEAT && s->ny % 64 == 0 && s->threads != 256;
     const bool f32 = s->dtype == PS_DTYPE_F32;
+    // Euler: faces shared between cells (threads = 256 keeps the per-cell kernel)
+    const bool euler_faces = s->eq == PS_EQ_EULER && s->threads != 256;
+    if (euler_faces) allow_big_smem(euler_standard_faces);
     if (f32 && !(fast && prm.i[0]))
         return fail(s, PS_ERR_UNSUPPORTED,
                     "float32 fields: heat with forward Euler and ny a multiple of 64 only");
@@ -553,6 +581,10 @@ int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_
                      else
                          heat_standard_fast<true><<<grid, 256, 0, s->stream>>>(
                              s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, gts, prm.d[0]);
+                 } else if (euler_faces) {
+                     const dim3 grid((s->ny + kEuTC - 1) / kEuTC, (s->nx + kEuTR - 1) / kEuTR);
+                     euler_standard_faces<<<grid, 256, kEuStdSmem, s->stream>>>(
+                         s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, gts, prm);
                  } else {
                      K(s->ring[c], s->ring[p], s->ring[n], fr, s->nx, s->ny, s->nv, gts, prm,
                        s->stream);
@@ -680,6 +712,7 @@ int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, i
         s->chunk = 64;
         if (stream_smem(s) > 227 * 1024) s->chunk = 32;
     }
+
     s->nseg = 1;
     if (rc == PS_OK) {
         cudaError_t e = cudaSetDevice(device);
@@ -968,6 +1001,7 @@ struct ps_batch {
     int device = 0, eq = 0, nv = 1, ops = 1, its = 1, bs = 0, mpss = 0, H = 0;
     int chunk = 32;  // column chunk of the generic streams (32 or 64)
     bool fast = false;
+    bool faces = false;  // Euler streams share faces (scratch beside the tile)
     cudaStream_t stream = nullptr;
     std::vector<BatchInst> inst;
     SweptArgs* d_desc = nullptr;  // [2 * count]: even / odd half-cycles
@@ -1062,12 +1096,18 @@ int batch_upload(ps_batch* b)
     return PS_OK;
 }
 
-size_t batch_stream_smem(const ps_batch* b)
+size_t batch_tile_smem(const ps_batch* b)
 {
-    if (b->fast) return b->bs == 16 ? heat_fast_smem<16>(b->H) : heat_fast_smem<32>(b->H);
     const int O2 = 2 * b->ops, RS = b->chunk + O2;
     return sizeof(double) * ((size_t)(b->its + 1) * b->nv * b->bs * RS +
                              (size_t)(b->H + 1) * b->nv * b->bs * O2);
+}
+
+size_t batch_stream_smem(const ps_batch* b)
+{
+    if (b->fast) return b->bs == 16 ? heat_fast_smem<16>(b->H) : heat_fast_smem<32>(b->H);
+    return batch_tile_smem(b) +
+           (b->faces ? sizeof(double) * euler_level_scratch(b->bs, b->chunk) : 0);
 }
 
 size_t batch_seam_smem(const ps_batch* b)
@@ -1137,7 +1177,8 @@ bool batch_pick(int eq, int ops, int its, int chunk, HalfFn* half, PrepFn* prep)
     PS_BSET(PS_EQ_HEAT, 1, 1, 32, Heat)
     PS_BSET(PS_EQ_HEAT, 1, 2, 32, Heat)
     PS_BSET(PS_EQ_EULER, 2, 2, 32, Euler)
-    PS_BSET(PS_EQ_EULER, 2, 2, 64, Euler)
+    PS_BSET(PS_EQ_EULER_CELL, 2, 2, 32, EulerCell)
+    PS_BSET(PS_EQ_EULER_CELL, 2, 2, 64, EulerCell)
     PS_BSET(PS_EQ_HALF, 1, 2, 32, Half)
 #undef PS_BSET
     return false;
@@ -1204,10 +1245,13 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
     b->mpss = blocksize / (2 * ops) - 1;
     b->H = b->mpss;
     b->fast = equation == PS_EQ_HEAT && its == 1 && (blocksize == 16 || blocksize == 32);
-    // Euler: 64-column chunks where the tile fits (as for a single solver)
+    // Euler: 64-column chunks where the tile fits, faces shared between cells
+    // where tile and scratch leave room for two CTAs per SM (as for a solver)
     if (!b->fast && equation == PS_EQ_EULER) {
         b->chunk = 64;
-        if (batch_stream_smem(b) > 227 * 1024) b->chunk = 32;
+        if (batch_tile_smem(b) > 227 * 1024) b->chunk = 32;
+        b->faces = batch_tile_smem(b) + sizeof(double) * euler_level_scratch(b->bs, b->chunk) <=
+                   kFaceSmemCap;
     }
     int rc = PS_OK;
     std::vector<int2> units;
@@ -1263,7 +1307,8 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
         if (e != cudaSuccess) rc = bfail(b, PS_ERR_NOMEM, "batch tables: %s", cudaGetErrorString(e));
     }
     // the kernels of the chosen chunk width (prep opts them into large shared memory)
-    if (rc == PS_OK && !batch_pick(equation, ops, its, b->chunk, &half, &prep))
+    const int keq = (equation == PS_EQ_EULER && !b->faces) ? PS_EQ_EULER_CELL : equation;
+    if (rc == PS_OK && !batch_pick(keq, ops, its, b->chunk, &half, &prep))
         rc = bfail(b, PS_ERR_UNSUPPORTED, "no batched kernels for chunk %d", b->chunk);
     if (rc == PS_OK) prep();
     if (rc != PS_OK) {
@@ -1334,7 +1379,8 @@ int ps_batch_run(ps_batch* b, int64_t nlevels, int use_graph)
     PSB_CUDA(b, cudaSetDevice(b->device));
     HalfFn half;
     PrepFn prep;
-    batch_pick(b->eq, b->ops, b->its, b->chunk, &half, &prep);
+    batch_pick((b->eq == PS_EQ_EULER && !b->faces) ? PS_EQ_EULER_CELL : b->eq, b->ops, b->its,
+               b->chunk, &half, &prep);
     const int64_t nhalf = (nlevels + b->H - 1) / b->H;
     if (!use_graph) {
         int rc = batch_upload(b);

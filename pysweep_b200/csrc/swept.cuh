@@ -98,6 +98,17 @@ __device__ __forceinline__ long long frame_slot(const SweptArgs& a, long long L)
     return s < a.frame_cap ? s : -1;
 }
 
+// Equations whose functor evaluates a whole stream level at once (faces
+// shared between cells): Eq::kFaceLevel and Eq::level<NT>.
+template <class Eq, class = void>
+struct FaceLevel {
+    static constexpr bool value = false;
+};
+template <class Eq>
+struct FaceLevel<Eq, decltype((void)Eq::kFaceLevel)> {
+    static constexpr bool value = Eq::kFaceLevel;
+};
+
 // ---------------------------------------------------------------- stream ----
 // One CTA = one (band, segment) block.  GAP = false: prism (UpPyramid);
 // GAP = true: gap (XBridge) centred on the band's upper boundary row.
@@ -166,7 +177,12 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
             const double* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
             const int gts = a.gts_base + (int)(a.L0 + m);
             // compute level m
-            {
+            if constexpr (FaceLevel<Eq>::value) {
+                // faces shared between the cells of the level (scratch after the carry)
+                Eq::template level<NT>(cur, prv, out, rlo, rhi, (klo > O2 ? klo : O2) - OPS,
+                                       RC - OPS, RS, BX, gts, a.p,
+                                       carry + (size_t)(a.Hmax + 1) * CS, tid);
+            } else {
                 const int k = O2 + tk;
                 if (k >= klo && k < RC) {
                     for (int i = rlo + tr; i < rhi; i += RG) {

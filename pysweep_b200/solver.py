@@ -215,14 +215,16 @@ class Solver:
             warnings.warn(f"share={self.share}: all rows run on the GPU (results do not depend "
                           "on the CPU/GPU split)")
         eqn = self.equation()
-        ic = np.asarray(self.initialConditions, dtype=np.float64)
+        # float32 fields (yaml `dtype: float32`) stay float32 on the device
+        fdt = np.dtype(np.float32) if self.dtype == np.float32 else np.dtype(np.float64)
+        ic = np.asarray(self.initialConditions, dtype=fdt)
         if ic.ndim == 2:
             ic = ic[None]
         nv, nx, ny = ic.shape
         self.createTimeStepData()
         self.moments.append(time.time())
         self.engine = Engine(eqn, nx, ny, nv=nv, ops=self.operating, its=self.intermediate,
-                             blocksize=self.blocksize[0], device=self.device)
+                             blocksize=self.blocksize[0], device=self.device, dtype=fdt.name)
         if self.tiling:
             self.engine.configure(**self.tiling)
         src = SourceModuleShim()
@@ -238,7 +240,8 @@ class Solver:
         every = max(1, self.output_every)
         # frames beyond the initial condition at full steps 1..nframes-1
         nkeep = (self.nframes - 1) // every
-        frames = np.empty((nkeep,) + ic.shape) if (self.write_output and nkeep) else None
+        frames = (np.empty((nkeep,) + ic.shape, dtype=fdt) if (self.write_output and nkeep)
+                  else None)
         mode = "swept" if self.simulation else "standard"
         self.engine.run(self.levels, mode=mode, frames=frames, frame_every=every)
         self.engine.synchronize()

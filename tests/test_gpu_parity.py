@@ -151,6 +151,25 @@ def test_euler_mass_conserved_and_decompositions_agree_at_256():
     assert abs(m1 - m0) / m0 < 1e-12
 
 
+@pytest.mark.parametrize("bs,cfg", [(16, {}), (16, {"chunk": 32}), (16, {"chunk": 32, "nseg": 4}),
+                                    (32, {}), (12, {"chunk": 32}), (8, {})])
+def test_euler_shared_faces_match_per_cell_step(bs, cfg):
+    """Euler's face-sharing kernels (standard tiles; stream levels where tile
+    and scratch fit two CTAs per SM: 32-column chunks at bs 16 and 12, bs 8)
+    against the per-cell step (threads = 256 selects the per-cell standard
+    kernel; 64-column chunks and bs 32 use it in the streams), the swept
+    decomposition and the oracle's x*x arithmetic, bitwise."""
+    n = 96 if bs == 12 else (64 if bs == 8 else 128)
+    steps = 7
+    ic, g = _ic_and_globals("euler", n, steps, None)
+    sw, swf = _gpu_frames("euler", ic, g, 2, 2, bs, steps * 2, "swept", **cfg)
+    st, stf = _gpu_frames("euler", ic, g, 2, 2, bs, steps * 2, "standard")
+    pc, pcf = _gpu_frames("euler", ic, g, 2, 2, bs, steps * 2, "standard", threads=256)
+    assert np.array_equal(st, pc) and np.array_equal(sw, st)
+    mul, _, _ = oracle.standard("euler", ic, g, 2, steps * 2, euler_square="mul")
+    assert np.array_equal(st, mul[: len(st)])
+
+
 FAST = [
     # n, bs, steps, tiling
     (128, 32, 45, {}),

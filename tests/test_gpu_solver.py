@@ -63,3 +63,32 @@ def test_command_line_heat_runs_swept_and_standard(tmp_path, monkeypatch):
     nlev = len(runs[False]) - 1
     _, want, _ = oracle.standard("heat", ic, s.globals, 1, nlev, frames=False)
     assert np.array_equal(runs[False][-1], want)
+
+
+@pytest.mark.parametrize("name", ["heat_fe_f32_n64_bs16", "heat_fe_f32_n128_bs32"])
+@pytest.mark.parametrize("swept", [True, False])
+def test_solver_yaml_float32_matches_reference_standard_frames(tmp_path, name, swept):
+    """`dtype: float32` in the yaml: float32 fields on the device, frames equal
+    to the reference's float32 standard frames bitwise (both decompositions;
+    the swept run keeps the reference's swept frame count)."""
+    import pysweep_b200
+    d = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    g = [float(x) for x in d["globals"]]
+    g[-1] = bool(g[-1])
+    cfg = {"swept": swept, "blocksize": int(d["bs"]), "share": 1, "intermediate_steps": 1,
+           "operating_points": 1, "globals": g, "cpu": os.path.join(EQDIR, "heat.py"),
+           "gpu": "heat.cu", "filename": str(tmp_path / "out.hdf5"), "dtype": "float32"}
+    yf = tmp_path / "in.yaml"
+    yf.write_text(yaml.dump(cfg))
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        s = pysweep_b200.Solver(d["ic"], str(yf))
+        s()
+    finally:
+        os.chdir(cwd)
+    assert s.data.dtype == np.float32 and s.final.dtype == np.float32
+    ref = d["standard"]
+    nf = len(d["swept"] if swept else ref)
+    assert s.data.shape == (nf,) + ref.shape[1:]
+    assert np.array_equal(s.data.astype(np.float64), ref[:nf])
