@@ -145,22 +145,6 @@ constexpr size_t heat_fast_smem(int hmax)
     return sizeof(double) * (size_t)kFastWarps * heat_fast_warp_doubles<BX>(hmax);
 }
 
-// 16-byte global -> shared copies that complete asynchronously (cp.async,
-// one commit group per level; wait_group<N> waits until at most N groups of
-// this thread are still in flight)
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-
-// 8-byte copy (cp.async.ca: the 4- and 8-byte sizes go through L1)
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-
 // one pair of T (16 bytes for double, 8 for float)
 template <class T>
 __device__ __forceinline__ void cp_async_pair(T* smem, const T* gmem)
@@ -169,17 +153,6 @@ __device__ __forceinline__ void cp_async_pair(T* smem, const T* gmem)
         cp_async16(smem, gmem);
     else
         cp_async8(smem, gmem);
-}
-
-__device__ __forceinline__ void cp_async_commit()
-{
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // A new cell pair from this lane's old rows (up u0, centre c0/c1, down d0)

@@ -148,7 +148,8 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
     const int units = nb * nseg;
     const int fgrid = (units + kFastWarps - 1) / kFastWarps;
     const size_t fsm = BX == 16 ? heat_fast_smem<16>(H) : heat_fast_smem<32>(H);
-    const size_t ssm = sizeof(double) * 2 * BX * (2 * (H + 1));
+    const size_t ssm = sizeof(double) * std::max(seam_smem_elems(false, BX, 1, 1, 1, H),
+                                                 seam_smem_elems(true, BX, 1, 1, 1, H));
     const int64_t halves = (nsteps + H - 1) / H;
     // outputs alternate between d_out and the scratch field so that the last
     // half-cycle lands in d_out and d_in is only read

@@ -387,8 +387,8 @@ size_t stream_smem(const ps_solver* s)
 
 size_t seam_smem(const ps_solver* s)
 {
-    const int TW = 2 * s->ops * (s->H + 1);
-    return s->esize * (size_t)(s->its + 1) * s->nv * s->bs * TW;
+    return s->esize * std::max(seam_smem_elems(false, s->bs, s->ops, s->nv, s->its, s->H),
+                               seam_smem_elems(true, s->bs, s->ops, s->nv, s->its, s->H));
 }
 
 int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t frame_cap,
@@ -1112,7 +1112,8 @@ size_t batch_stream_smem(const ps_batch* b)
 
 size_t batch_seam_smem(const ps_batch* b)
 {
-    return sizeof(double) * (size_t)(b->its + 1) * b->nv * b->bs * (2 * b->ops * (b->H + 1));
+    return sizeof(double) * std::max(seam_smem_elems(false, b->bs, b->ops, b->nv, b->its, b->H),
+                                     seam_smem_elems(true, b->bs, b->ops, b->nv, b->its, b->H));
 }
 
 using BatchFast = void (*)(const SweptArgs*, const int2*, int, int, int, long long);
@@ -1281,6 +1282,9 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
         for (int u = 0; u < I.nb * I.nseg; ++u) units.push_back(make_int2(i, u));
         b->inst.push_back(I);
     }
+    if (rc == PS_OK && batch_seam_smem(b) > 227 * 1024)
+        rc = bfail(b, PS_ERR_UNSUPPORTED, "seam tile needs %zu bytes of shared memory",
+                   batch_seam_smem(b));
     if (rc == PS_OK) {
         cudaError_t e = cudaSetDevice(device);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);

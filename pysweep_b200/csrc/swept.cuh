@@ -88,6 +88,80 @@ __device__ __forceinline__ int seg_start(const SweptArgs& a, int s)
     return a.seg_unit * (int)(((long long)s * a.seg_units) / a.nseg);
 }
 
+// Global -> shared copies that complete asynchronously (cp.async; one
+// commit group per batch, wait_group<N> waits until at most N groups of this
+// thread are still in flight).  16 bytes bypass L1 (.cg); 4 and 8 go through
+// it (.ca, the only form for those sizes).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// one element of T (8 bytes for double, 4 for float)
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem)
+{
+    if constexpr (sizeof(T) == 8)
+        cp_async8(smem, gmem);
+    else
+        cp_async4(smem, gmem);
+}
+
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Seam kernels stage the faces of every level of the half-cycle in shared
+// memory before the first level (the stream kernels wrote them all before
+// the seam launch), so no level waits on a global load.  Per level m the
+// staged y-faces are nv*nr*2OPS values per side (nr: the level's rows), the
+// gap's staged x-face rows nv*2*2OPS*(2*OPS*m + 2*2OPS) values.
+__host__ __device__ inline int seam_rows(bool gap, int bx, int ops, int m)
+{
+    return gap ? 2 * ops * m : bx - 2 * ops * m;
+}
+// staged y-face values of levels 1 .. m-1 (both sides)
+__host__ __device__ inline int seam_yoff(bool gap, int bx, int ops, int nv, int m)
+{
+    // sum over levels 1..m-1 of 2 * nv * rows * 2OPS
+    const int rows = gap ? ops * m * (m - 1) : (m - 1) * bx - ops * m * (m - 1);
+    return 2 * nv * 2 * ops * rows;
+}
+// staged x-face values of levels 1 .. m-1 (gap only)
+__host__ __device__ inline int seam_xoff(int ops, int nv, int m)
+{
+    // sum over levels 1..m-1 of nv * 2 * 2OPS * (2*OPS*m' + 2*2OPS)
+    return nv * 4 * ops * (ops * m * (m - 1) + 4 * ops * (m - 1));
+}
+// Shared memory of one seam CTA in elements: its+1 tile slots, then the
+// staged faces of levels 1 .. hmax-1.
+__host__ __device__ inline size_t seam_smem_elems(bool gap, int bx, int ops, int nv, int its,
+                                                  int hmax)
+{
+    const size_t slots = (size_t)(its + 1) * nv * bx * (2 * ops * (hmax + 1));
+    return slots + seam_yoff(gap, bx, ops, nv, hmax) + (gap ? seam_xoff(ops, nv, hmax) : 0);
+}
+
 // Frame slot for global level L, or -1.
 __device__ __forceinline__ long long frame_slot(const SweptArgs& a, long long L)
 {
@@ -355,6 +429,42 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
             }
         }
     }
+    // faces of levels 1 .. H-1, staged in the loops' own element order: the
+    // y-faces (left side, then right side) and, in the gap, the prisms' rows
+    // around it
+    T* ystage = slot + NSLOT * SL;
+    T* xstage = ystage + seam_yoff(GAP, BX, OPS, nv, a.Hmax);
+    for (int m = 1; m <= H - 1; ++m) {
+        const int rlo = GAP ? hx - OPS * m : OPS * m;
+        const int nr = seam_rows(GAP, BX, OPS, m), n = nv * nr * O2;
+        const T* yl = yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
+        const T* yr = yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
+        T* ys = ystage + seam_yoff(GAP, BX, OPS, nv, m);
+        for (int e = tid; e < n; e += NT) {
+            const int j = e % O2, t = e / O2;
+            const int i = rlo + t % nr, v = t / nr;
+            cp_async_elem(ys + e, yl + (v * BX + i) * O2 + j);
+            cp_async_elem(ys + n + e, yr + (v * BX + i) * O2 + j);
+        }
+        if (GAP) {
+            const int clo = KC - OPS * m;
+            const int nc = 2 * OPS * m + 2 * O2;
+            const int n2 = nv * 2 * O2 * nc;
+            const int bup = wrap(band - 1, a.nb), bdn = band;
+            T* xs = xstage + seam_xoff(OPS, nv, m);
+            for (int e = tid; e < n2; e += NT) {
+                const int k = clo - O2 + e % nc, t = e / nc;
+                const int rr = t % (2 * O2), v = t / (2 * O2);
+                const int side = rr < O2 ? 1 : 0;
+                const int j = rr < O2 ? rr : rr - O2;
+                const int bb = rr < O2 ? bup : bdn;
+                const size_t fo = ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                cp_async_elem(xs + e, xface + fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny));
+            }
+        }
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     for (int m = 1; m <= H; ++m) {
         const int rlo = GAP ? hx - OPS * m : OPS * m;
@@ -376,29 +486,24 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
             // y-faces of level m: left part from the left block's right edge,
             // right part from the right block's left edge.
             const int nr = rhi - rlo, n = nv * nr * O2;
-            const T* yl = yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
-            const T* yr = yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
+            const T* ys = ystage + seam_yoff(GAP, BX, OPS, nv, m);
             for (int e = tid; e < n; e += NT) {
                 const int j = e % O2, t = e / O2;
                 const int i = rlo + t % nr, v = t / nr;
-                out[(v * BX + i) * TW + clo - O2 + j] = yl[(v * BX + i) * O2 + j];
-                out[(v * BX + i) * TW + chi + j] = yr[(v * BX + i) * O2 + j];
+                out[(v * BX + i) * TW + clo - O2 + j] = ys[e];
+                out[(v * BX + i) * TW + chi + j] = ys[n + e];
             }
             if (GAP) {
                 // the prisms' rows around the gap, columns [clo-2OPS, chi+2OPS)
                 const int nc = chi - clo + 2 * O2;
                 const int n2 = nv * 2 * O2 * nc;
-                const int bup = wrap(band - 1, a.nb), bdn = band;
+                const T* xs = xstage + seam_xoff(OPS, nv, m);
                 for (int e = tid; e < n2; e += NT) {
                     const int k = clo - O2 + e % nc, t = e / nc;
                     const int rr = t % (2 * O2), v = t / (2 * O2);
-                    const int side = rr < O2 ? 1 : 0;
                     const int j = rr < O2 ? rr : rr - O2;
                     const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
-                    const int bb = rr < O2 ? bup : bdn;
-                    const size_t fo =
-                        ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                    out[(v * BX + i) * TW + k] = xface[fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny)];
+                    out[(v * BX + i) * TW + k] = xs[e];
                 }
             }
         }
