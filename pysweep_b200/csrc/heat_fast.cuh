@@ -240,33 +240,46 @@ __device__ __forceinline__ void store_bottom(int count, const double (&a0)[BX],
 }
 #undef PSB_BOTTOM_CASE
 
-// Gap: rows K and K-1 of level m (K odd).  Row K takes its left neighbours
-// from the arrays and the carry; row K-1 reuses two of them (the old rows
-// K-2 and K-1 are not written by row K), so a pair needs six shuffles.
+// Gap: rows K and K-1 of level m (K odd), in place and descending (row k
+// reads old rows k-2, k-1, k).  On entry L1a, L1b hold the left neighbours
+// of old rows K and K-1 (column 1 of the lane to the left, or the carry for
+// lane 0); on exit those of old rows K-2 and K-3, which the next pair needs
+// (old rows below K-1 are not written by this pair), so a pair takes four
+// new shuffles.
 template <int K, int BX, class T>
 __device__ __forceinline__ void gap_pair(double (&a0)[BX], double (&a1)[BX], const double* cr0,
-                                         int lane, double cr)
+                                         int lane, double cr, double& L1a, double& L1b)
 {
     if constexpr (K >= 3 && K < BX) {
+        const double L1d = L1a, L1c = L1b;
         const double2 cu = *reinterpret_cast<const double2*>(cr0 + (K - 2) * 2);
-        const double2 cc = *reinterpret_cast<const double2*>(cr0 + (K - 1) * 2);
-        const double2 cd = *reinterpret_cast<const double2*>(cr0 + K * 2);
         const double L1u = from_left(a1[K - 2], cu.y, lane);
-        const double L1c = from_left(a1[K - 1], cc.y, lane);
-        const double L1d = from_left(a1[K], cd.y, lane);
-        const double L0c = from_left(a0[K - 1], cc.x, lane);
+        const double L0c = from_left(a0[K - 1], cr0[(K - 1) * 2], lane);
         double n0, n1;
         heat_pair<T>(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], cr, n0, n1);
         a0[K] = n0;
         a1[K] = n1;
         // row K-1: up K-3, centre K-2, down K-1
-        const double2 cuu = *reinterpret_cast<const double2*>(cr0 + (K - 3) * 2);
-        const double L1uu = from_left(a1[K - 3], cuu.y, lane);
+        const double L1uu = from_left(a1[K - 3], cr0[(K - 3) * 2 + 1], lane);
         const double L0cc = from_left(a0[K - 2], cu.x, lane);
         heat_pair<T>(L1uu, L1u, L1c, L0cc, a0[K - 3], a0[K - 2], a0[K - 1], a1[K - 2], cr, n0,
                      n1);
         a0[K - 1] = n0;
         a1[K - 1] = n1;
+        L1a = L1u;
+        L1b = L1uu;
+    }
+}
+
+// Gap: the left neighbours of old rows K and K-1, which the level's first
+// pair takes on entry.
+template <int K, int BX>
+__device__ __forceinline__ void gap_entry(const double (&a1)[BX], const double* cr0, int lane,
+                                          double& L1a, double& L1b)
+{
+    if constexpr (K >= 3 && K < BX) {
+        L1a = from_left(a1[K], cr0[K * 2 + 1], lane);
+        L1b = from_left(a1[K - 1], cr0[(K - 1) * 2 + 1], lane);
     }
 }
 
@@ -397,56 +410,31 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
                 // k-2 (up), k-1 (centre), k (down).
                 const int K0 = 2 * m + 1;
                 nrow = 2 * m + 2;
-                // rows K0 .. 2, entered at K0 = 2m+1 and falling through
+                // rows K0 .. 2, entered at K0 = 2m+1 (a prologue takes the first
+                // pair's two carried neighbours) and falling through
+                double L1a = 0.0, L1b = 0.0;
+#define PSB_GAP_ENTRY(K)                                                                   \
+    case K:                                                                                \
+        gap_entry<K, BX>(a1, cr0, lane, L1a, L1b);                                         \
+        goto pair_##K;
+#define PSB_GAP_PAIR(K)                                                                    \
+    pair_##K:                                                                              \
+    gap_pair<K, BX, T>(a0, a1, cr0, lane, cr, L1a, L1b);
                 switch (K0) {
-                case 31:
-                    gap_pair<31, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 29:
-                    gap_pair<29, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 27:
-                    gap_pair<27, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 25:
-                    gap_pair<25, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 23:
-                    gap_pair<23, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 21:
-                    gap_pair<21, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 19:
-                    gap_pair<19, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 17:
-                    gap_pair<17, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 15:
-                    gap_pair<15, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 13:
-                    gap_pair<13, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 11:
-                    gap_pair<11, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 9:
-                    gap_pair<9, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 7:
-                    gap_pair<7, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 5:
-                    gap_pair<5, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
-                case 3:
-                    gap_pair<3, BX, T>(a0, a1, cr0, lane, cr);
-                    [[fallthrough]];
+                    PSB_GAP_ENTRY(31) PSB_GAP_ENTRY(29) PSB_GAP_ENTRY(27) PSB_GAP_ENTRY(25)
+                    PSB_GAP_ENTRY(23) PSB_GAP_ENTRY(21) PSB_GAP_ENTRY(19) PSB_GAP_ENTRY(17)
+                    PSB_GAP_ENTRY(15) PSB_GAP_ENTRY(13) PSB_GAP_ENTRY(11) PSB_GAP_ENTRY(9)
+                    PSB_GAP_ENTRY(7) PSB_GAP_ENTRY(5) PSB_GAP_ENTRY(3)
                 default:
-                    break;
+                    goto pairs_done;
                 }
+                PSB_GAP_PAIR(31) PSB_GAP_PAIR(29) PSB_GAP_PAIR(27) PSB_GAP_PAIR(25)
+                PSB_GAP_PAIR(23) PSB_GAP_PAIR(21) PSB_GAP_PAIR(19) PSB_GAP_PAIR(17)
+                PSB_GAP_PAIR(15) PSB_GAP_PAIR(13) PSB_GAP_PAIR(11) PSB_GAP_PAIR(9)
+                PSB_GAP_PAIR(7) PSB_GAP_PAIR(5) PSB_GAP_PAIR(3)
+            pairs_done:
+#undef PSB_GAP_ENTRY
+#undef PSB_GAP_PAIR
                 // the face rows of level m join: upper at indices 0, 1, lower at
                 // 2m+2, 2m+3 (the next level's first centre and down rows).
                 // Each lane reads back only the pairs it copied.
