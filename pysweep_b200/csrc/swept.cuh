@@ -379,6 +379,28 @@ __global__ void __launch_bounds__(NT) stream_kernel(SweptArgs a)
 // One CTA per (band, segment): the column edge at x0 = seg*wy between segment
 // seg-1 (left) and seg (right).  GAP = false: YBridge; GAP = true: the
 // Octahedron's down half.  Tile columns k <-> global x0 - KC + k, KC = OPS*(Hmax+1).
+// ceil(log2(n)) for n >= 1
+__device__ __forceinline__ int log2_ceil(int n)
+{
+    return n <= 1 ? 0 : 32 - __clz(n - 1);
+}
+
+// f(r, c) for every (r, c) in [0, nr) x [0, nc), spread over NT threads:
+// c from the low bits of the thread index (a power-of-two group of at least
+// nc threads, at most NT), r strided by the number of groups.  Masks and
+// shifts only: no division by the run-time extents.
+template <int NT, class F>
+__device__ __forceinline__ void for_2d(int nr, int nc, int tid, F&& f)
+{
+    static_assert((NT & (NT - 1)) == 0, "NT is a power of two");
+    constexpr int kLogNT = 31 - __builtin_clz(NT);
+    const int lg = min(log2_ceil(nc), kLogNT);
+    const int cw = 1 << lg;
+    const int c0 = tid & (cw - 1), rs = NT >> lg;
+    for (int c = c0; c < nc; c += cw)
+        for (int r = tid >> lg; r < nr; r += rs) f(r, c);
+}
+
 template <class Eq, int ITS, bool GAP, int NT, class T = double>
 __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T* sm)
 {
@@ -396,8 +418,20 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
     const int ul = band * a.nseg + (seg + a.nseg - 1) % a.nseg;  // left stream unit
     const int ur = unit;                                          // right stream unit
+    const int bup = wrap(band - 1, a.nb);
     const int tid = threadIdx.x;
     const int HF = a.Hmax - 1;
+    // grid row of tile row i and grid column of tile column k (BX <= nx and
+    // TW <= ny, so one wrap at most)
+    const int rbase = wrap(r0, nx), cbase = wrap(x0 - KC, ny);
+    auto grow = [&](int i) {
+        const int r = rbase + i;
+        return r >= nx ? r - nx : r;
+    };
+    auto gcol = [&](int k) {
+        const int c = cbase + k;
+        return c >= ny ? c - ny : c;
+    };
     Nbr nb;
     nb.vs = BX * TW;
 #pragma unroll
@@ -409,29 +443,25 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
     {
         const int lo0 = GAP ? hx - O2 : 0, hi0 = GAP ? hx + O2 : BX;
         const T* b0 = bin + (size_t)(ITS - 1) * nv * nx * ny;
-        const int nr = hi0 - lo0, n = nv * nr * 2 * O2;
-        for (int e = tid; e < n; e += NT) {
-            const int k = KC - O2 + e % (2 * O2), t = e / (2 * O2);
-            const int i = lo0 + t % nr, v = t / nr;
-            slot[(v * BX + i) * TW + k] =
-                b0[((size_t)v * nx + wrap(r0 + i, nx)) * ny + wrap(x0 - KC + k, ny)];
-        }
+        for (int v = 0; v < nv; ++v)
+            for_2d<NT>(hi0 - lo0, 2 * O2, tid, [&](int r, int c) {
+                const int i = lo0 + r, k = KC - O2 + c;
+                slot[(v * BX + i) * TW + k] = b0[((size_t)v * nx + grow(i)) * ny + gcol(k)];
+            });
         if (ITS >= 2) {
             const int lo1 = GAP ? hx - OPS : OPS, hi1 = GAP ? hx + OPS : BX - OPS;
             const T* b1 = bin + (size_t)(ITS - 2) * nv * nx * ny;
             T* s1p = slot + (NSLOT - 1) * SL;
-            const int nr1 = hi1 - lo1, n1 = nv * nr1 * O2;
-            for (int e = tid; e < n1; e += NT) {
-                const int k = KC - OPS + e % O2, t = e / O2;
-                const int i = lo1 + t % nr1, v = t / nr1;
-                s1p[(v * BX + i) * TW + k] =
-                    b1[((size_t)v * nx + wrap(r0 + i, nx)) * ny + wrap(x0 - KC + k, ny)];
-            }
+            for (int v = 0; v < nv; ++v)
+                for_2d<NT>(hi1 - lo1, O2, tid, [&](int r, int c) {
+                    const int i = lo1 + r, k = KC - OPS + c;
+                    s1p[(v * BX + i) * TW + k] = b1[((size_t)v * nx + grow(i)) * ny + gcol(k)];
+                });
         }
     }
-    // faces of levels 1 .. H-1, staged in the loops' own element order: the
-    // y-faces (left side, then right side) and, in the gap, the prisms' rows
-    // around it
+    // faces of levels 1 .. H-1, staged: per level the y-faces
+    // [side][v][row][j] (left block's right edge, then right block's left
+    // edge) and, in the gap, the prisms' rows around it [v][rr][column]
     T* ystage = slot + NSLOT * SL;
     T* xstage = ystage + seam_yoff(GAP, BX, OPS, nv, a.Hmax);
     for (int m = 1; m <= H - 1; ++m) {
@@ -440,27 +470,27 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
         const T* yl = yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
         const T* yr = yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
         T* ys = ystage + seam_yoff(GAP, BX, OPS, nv, m);
-        for (int e = tid; e < n; e += NT) {
-            const int j = e % O2, t = e / O2;
-            const int i = rlo + t % nr, v = t / nr;
-            cp_async_elem(ys + e, yl + (v * BX + i) * O2 + j);
-            cp_async_elem(ys + n + e, yr + (v * BX + i) * O2 + j);
-        }
+        for (int v = 0; v < nv; ++v)
+            for_2d<NT>(nr, O2, tid, [&](int r, int j) {
+                const int e = (v * nr + r) * O2 + j;
+                const int src = (v * BX + rlo + r) * O2 + j;
+                cp_async_elem(ys + e, yl + src);
+                cp_async_elem(ys + n + e, yr + src);
+            });
         if (GAP) {
             const int clo = KC - OPS * m;
             const int nc = 2 * OPS * m + 2 * O2;
-            const int n2 = nv * 2 * O2 * nc;
-            const int bup = wrap(band - 1, a.nb), bdn = band;
             T* xs = xstage + seam_xoff(OPS, nv, m);
-            for (int e = tid; e < n2; e += NT) {
-                const int k = clo - O2 + e % nc, t = e / nc;
-                const int rr = t % (2 * O2), v = t / (2 * O2);
-                const int side = rr < O2 ? 1 : 0;
-                const int j = rr < O2 ? rr : rr - O2;
-                const int bb = rr < O2 ? bup : bdn;
-                const size_t fo = ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                cp_async_elem(xs + e, xface + fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny));
-            }
+            for (int v = 0; v < nv; ++v)
+                for_2d<NT>(2 * O2, nc, tid, [&](int rr, int kk) {
+                    const int side = rr < O2 ? 1 : 0;
+                    const int j = rr < O2 ? rr : rr - O2;
+                    const int bb = rr < O2 ? bup : band;
+                    const size_t fo =
+                        ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                    cp_async_elem(xs + (v * 2 * O2 + rr) * nc + kk,
+                                  xface + fo * ny + xface_col(gcol(clo - O2 + kk), m, ny));
+                });
         }
     }
     cp_async_commit();
@@ -470,78 +500,67 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
         const int rlo = GAP ? hx - OPS * m : OPS * m;
         const int rhi = GAP ? hx + OPS * m : BX - OPS * m;
         const int clo = KC - OPS * m, chi = KC + OPS * m;
+        const int nr = rhi - rlo, nc = chi - clo;
         T* out = slot + (m % NSLOT) * SL;
         const T* cur = slot + ((m - 1) % NSLOT) * SL;
         const T* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
         const int gts = a.gts_base + (int)(a.L0 + m);
-        {
-            const int nc = chi - clo, nr = rhi - rlo;
-            for (int e = tid; e < nr * nc; e += NT) {
-                const int k = clo + e % nc, i = rlo + e / nc;
-                const int o = i * TW + k;
-                Eq::step(cur + o, prv + o, out + o, nb, gts, nv, a.p);
-            }
-        }
+        for_2d<NT>(nr, nc, tid, [&](int r, int c) {
+            const int o = (rlo + r) * TW + clo + c;
+            Eq::step(cur + o, prv + o, out + o, nb, gts, nv, a.p);
+        });
         if (m <= H - 1) {
             // y-faces of level m: left part from the left block's right edge,
             // right part from the right block's left edge.
-            const int nr = rhi - rlo, n = nv * nr * O2;
+            const int n = nv * nr * O2;
             const T* ys = ystage + seam_yoff(GAP, BX, OPS, nv, m);
-            for (int e = tid; e < n; e += NT) {
-                const int j = e % O2, t = e / O2;
-                const int i = rlo + t % nr, v = t / nr;
-                out[(v * BX + i) * TW + clo - O2 + j] = ys[e];
-                out[(v * BX + i) * TW + chi + j] = ys[n + e];
-            }
+            for (int v = 0; v < nv; ++v)
+                for_2d<NT>(nr, O2, tid, [&](int r, int j) {
+                    const int e = (v * nr + r) * O2 + j;
+                    T* row = out + (v * BX + rlo + r) * TW;
+                    row[clo - O2 + j] = ys[e];
+                    row[chi + j] = ys[n + e];
+                });
             if (GAP) {
                 // the prisms' rows around the gap, columns [clo-2OPS, chi+2OPS)
-                const int nc = chi - clo + 2 * O2;
-                const int n2 = nv * 2 * O2 * nc;
+                const int nc2 = nc + 2 * O2;
                 const T* xs = xstage + seam_xoff(OPS, nv, m);
-                for (int e = tid; e < n2; e += NT) {
-                    const int k = clo - O2 + e % nc, t = e / nc;
-                    const int rr = t % (2 * O2), v = t / (2 * O2);
-                    const int j = rr < O2 ? rr : rr - O2;
-                    const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
-                    out[(v * BX + i) * TW + k] = xs[e];
-                }
+                for (int v = 0; v < nv; ++v)
+                    for_2d<NT>(2 * O2, nc2, tid, [&](int rr, int kk) {
+                        const int j = rr < O2 ? rr : rr - O2;
+                        const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
+                        out[(v * BX + i) * TW + clo - O2 + kk] = xs[(v * 2 * O2 + rr) * nc2 + kk];
+                    });
             }
         }
         __syncthreads();
         // outputs of level m
-        {
-            const long long L = a.L0 + m;
-            const int nc = chi - clo;
-            if (!GAP && m <= H - 1) {
-                const int n = nv * 2 * O2 * nc;
-                for (int e = tid; e < n; e += NT) {
-                    const int k = clo + e % nc, t = e / nc;
-                    const int rr = t % (2 * O2), v = t / (2 * O2);
+        if (!GAP && m <= H - 1) {
+            for (int v = 0; v < nv; ++v)
+                for_2d<NT>(2 * O2, nc, tid, [&](int rr, int kk) {
                     const int side = rr < O2 ? 0 : 1;
                     const int j = rr < O2 ? rr : rr - O2;
                     const int i = side == 0 ? OPS * m + j : BX - OPS * m - O2 + j;
+                    const int k = clo + kk;
                     const size_t fo =
                         ((((size_t)band * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                    xface[fo * ny + xface_col(wrap(x0 - KC + k, ny), m, ny)] = out[(v * BX + i) * TW + k];
-                }
-            }
-            const bool tob = m > H - ITS;
-            const long long fs = frame_slot(a, L);
-            if (tob || fs >= 0) {
-                const int nr = rhi - rlo, n = nv * nr * nc;
-                T* bo = tob ? reinterpret_cast<T*>(a.bout) + (size_t)(m - (H - ITS) - 1) * nv * nx * ny
-                            : nullptr;
-                T* fr = fs >= 0 ? reinterpret_cast<T*>(a.frames) + (size_t)fs * nv * nx * ny : nullptr;
-                for (int e = tid; e < n; e += NT) {
-                    const int k = clo + e % nc, t = e / nc;
-                    const int i = rlo + t % nr, v = t / nr;
+                    xface[fo * ny + xface_col(gcol(k), m, ny)] = out[(v * BX + i) * TW + k];
+                });
+        }
+        const bool tob = m > H - ITS;
+        const long long fs = frame_slot(a, a.L0 + m);
+        if (tob || fs >= 0) {
+            T* bo = tob ? reinterpret_cast<T*>(a.bout) + (size_t)(m - (H - ITS) - 1) * nv * nx * ny
+                        : nullptr;
+            T* fr = fs >= 0 ? reinterpret_cast<T*>(a.frames) + (size_t)fs * nv * nx * ny : nullptr;
+            for (int v = 0; v < nv; ++v)
+                for_2d<NT>(nr, nc, tid, [&](int r, int kk) {
+                    const int i = rlo + r, k = clo + kk;
                     const T val = out[(v * BX + i) * TW + k];
-                    const size_t go =
-                        ((size_t)v * nx + wrap(r0 + i, nx)) * ny + wrap(x0 - KC + k, ny);
+                    const size_t go = ((size_t)v * nx + grow(i)) * ny + gcol(k);
                     if (bo) bo[go] = val;
                     if (fr) fr[go] = val;
-                }
-            }
+                });
         }
     }
 }
