@@ -67,6 +67,10 @@ struct ps_solver {
     bool nseg_auto = true;  // choose the segment count per run until configured
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // the gap stream runs beside the y-bridge seam on a high-priority side
+    // stream (forked from and joined back into `stream` with two events)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // named plugin constants
     std::map<std::string, double> globals;
     // device buffers
@@ -304,18 +308,19 @@ cudaEvent_t take_event(ps_solver* s)
 // Kernel kinds for ps_profile_read: 0 prism stream, 1 Y-bridge seam, 2 gap
 // stream, 3 octahedron seam, 4 standard step.
 template <class F>
-int timed_launch(ps_solver* s, int kind, double cells, F&& launch)
+int timed_launch(ps_solver* s, int kind, double cells, F&& launch, cudaStream_t st = nullptr)
 {
     cudaEvent_t a = nullptr, b = nullptr;
+    if (!st) st = s->stream;
     if (s->profile) {
         a = take_event(s);
         b = take_event(s);
-        cudaEventRecord(a, s->stream);
+        cudaEventRecord(a, st);
     }
     launch();
     int rc = check_launch(s);
     if (s->profile) {
-        cudaEventRecord(b, s->stream);
+        cudaEventRecord(b, st);
         s->pending.push_back({kind, {a, b}});
         s->prof_cells[kind] += cells;
     }
@@ -343,7 +348,9 @@ int ensure_swept_buffers(ps_solver* s)
     const int nb = s->nx / s->bs;
     const int HF = std::max(s->H - 1, 0);
     const size_t xn = (size_t)nb * HF * 2 * s->nv * O2 * s->ny;
-    const size_t yn = (size_t)nb * s->nseg * 2 * HF * s->nv * s->bs * O2;
+    // two y-face buffers: prism -> y-bridge, gap -> octahedron (the y-bridge
+    // and the gap stream run at the same time)
+    const size_t yn = 2 * (size_t)nb * s->nseg * 2 * HF * s->nv * s->bs * O2;
     if (xn > s->xface_n) {
         if (s->xface) cudaFree(s->xface);
         s->xface = nullptr;
@@ -466,6 +473,13 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         return fail(s, PS_ERR_UNSUPPORTED, "tile needs %zu bytes of shared memory", smem);
     int rc = ensure_swept_buffers(s);
     if (rc) return rc;
+    if (!s->side) {
+        int lo = 0, hi = 0;
+        PS_CUDA(s, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        PS_CUDA(s, cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi));
+        PS_CUDA(s, cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+        PS_CUDA(s, cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+    }
     SweptArgs a;
     memset(&a, 0, sizeof a);
     a.frames = frames;
@@ -522,10 +536,19 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         const double u = (double)a.nb;
         const size_t psm = K.fast ? (s->bs == 16 ? heat_fast_smem<16>(s->H) : heat_fast_smem<32>(s->H))
                                   : stream_smem(s);
+        // P, then Y on `stream` beside G on the side stream (G reads nothing
+        // that Y writes: its valid cells depend on the prisms' faces only,
+        // and it writes its y-faces into the second buffer), then O
+        SweptArgs ag = a;
+        ag.yface = at(s, s->yface, s->yface_n / 2);
         if ((rc = timed_launch(s, 0, cP * u, [&] { K.P(a, units, psm, s->stream); }))) return rc;
+        PS_CUDA(s, cudaEventRecord(s->ev_fork, s->stream));
+        PS_CUDA(s, cudaStreamWaitEvent(s->side, s->ev_fork, 0));
+        if ((rc = timed_launch(s, 2, cG * u, [&] { K.G(ag, units, psm, s->side); }, s->side))) return rc;
+        PS_CUDA(s, cudaEventRecord(s->ev_join, s->side));
         if ((rc = timed_launch(s, 1, cY * u, [&] { K.Y(a, units, seam_smem(s), s->stream); }))) return rc;
-        if ((rc = timed_launch(s, 2, cG * u, [&] { K.G(a, units, psm, s->stream); }))) return rc;
-        if ((rc = timed_launch(s, 3, cO * u, [&] { K.O(a, units, seam_smem(s), s->stream); }))) return rc;
+        PS_CUDA(s, cudaStreamWaitEvent(s->stream, s->ev_join, 0));
+        if ((rc = timed_launch(s, 3, cO * u, [&] { K.O(ag, units, seam_smem(s), s->stream); }))) return rc;
         s->cur = 1 - s->cur;
         off = ((off - a.hx) % s->nx + s->nx) % s->nx;
         done += H;
@@ -755,6 +778,12 @@ int ps_destroy(ps_solver* s)
         cudaEventDestroy(p.second.second);
     }
     for (auto e : s->event_pool) cudaEventDestroy(e);
+    if (s->side) {
+        cudaStreamSynchronize(s->side);
+        cudaStreamDestroy(s->side);
+    }
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return PS_OK;
