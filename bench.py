@@ -134,6 +134,23 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+FP64_OPS_PER_CELL = 8   # heat, forward Euler: 2 FMA, 4 add, 2 multiply (numpy's order)
+FP64_LANES_PER_SM = 64  # B200: 148 SMs x 64 FP64 lanes x 1965 MHz = 18.6 T FP64 instructions/s
+
+
+def fp64_roof(cells, ms, clk):
+    """The swept streams are bound by FP64 issue, not HBM: FP64 instructions
+    per second of the dominant kernel against the FP64 pipe's rate at the
+    sampled SM clock (an FMA counts as one instruction)."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    achieved = cells * FP64_OPS_PER_CELL / (ms / 1000) / 1e9
+    peak = sms * FP64_LANES_PER_SM * mhz * 1e6 / 1e9
+    return {"ops_per_cell": FP64_OPS_PER_CELL, "achieved_ginstr_s": achieved,
+            "peak_ginstr_s": peak, "frac": achieved / peak, "sm_mhz": mhz}
+
+
 def ncu_traffic(kind, n, bs):
     """DRAM bytes per launch of one kernel kind, from a committed ncu summary."""
     p = os.path.join(ROOT, "profiles", f"heat2d_swept_{kind}_traffic.txt")
@@ -313,7 +330,8 @@ def run_b200(args):
             "launches": dn, "avg_launch_ms": dms / dn,
             "algorithmic_bytes_per_launch": dcells * cell_bytes / dn,
             "peak_source": peak_src,
-            "kernel_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()}}
+            "kernel_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()},
+            "fp64": fp64_roof(dcells, dms, clk)}
 
     cfg = workload_config(args)
     if f32:

@@ -76,6 +76,7 @@ CONFIGS = [
     ("heat", 96, 24, 1, 2, 25, False, {"nseg": 2}),
     ("heat", 80, 8, 1, 1, 17, True, {"chunk": 64}),
     ("euler", 64, 16, 2, 2, 12, None, {}),
+    ("euler", 64, 16, 2, 2, 11, None, {"nseg": 1}),
     ("euler", 64, 32, 2, 2, 10, None, {"nseg": 2}),
     ("euler", 96, 16, 2, 2, 9, None, {"h": 2, "nseg": 3}),
     ("euler", 128, 16, 2, 2, 9, None, {"chunk": 64}),
@@ -181,6 +182,7 @@ FAST = [
     (256, 32, 33, {"nseg": 3}),   # uneven segments: 1, 1 and 2 chunks
     (320, 16, 17, {"nseg": 4}),   # 5 chunks over 4 segments
     (384, 32, 40, {"nseg": 0}),   # automatic segment count
+    (256, 32, 37, {"nseg": 1}),   # one segment: each seam joins a block to itself
 ]
 
 
