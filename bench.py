@@ -208,8 +208,6 @@ def run_reference(args):
 def workload_config(args):
     return {"workload": f"heat2d-fp64-periodic-{args.n}x{args.n}-{args.nsteps}steps-swept",
             "n": args.n, "time_steps": args.nsteps, "blocksize": args.bs,
-            "levels_per_half_cycle": args.h or args.bs // 2 - 1,
-            "nseg": args.nseg or "auto (one wave of warps)",
             "l2": "inputs larger than L2 (field of n*n*8 bytes)"}
 
 
@@ -342,7 +340,8 @@ def run_b200(args):
             "dtype": "f32 storage, f64 arithmetic" if f32 else "f64",
             "data": "synthetic", "config": cfg, "standard": std,
             "swept_vs_standard": (value / std["value"]) if std else None,
-            "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches}
+            "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+            "tiling": dict(eng.tiling(), nseg_auto=not args.nseg)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not f32:
         threads = os.cpu_count() or 1
         v, secs = cpu_baseline(args.ref_n, bs, args.ref_cycles, threads)
@@ -449,7 +448,8 @@ def run_b200_slabs(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_sw,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": cfg, "standard": None, "swept_vs_standard": None,
-            "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches}
+            "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+            "tiling": dict(eng.tiling(), nseg_auto=not args.nseg)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     sol.close()

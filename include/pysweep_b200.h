@@ -105,9 +105,20 @@ int ps_get_global_value(ps_solver *s, const char *name, double *value);
  * chunk = streaming chunk width (32 or 64) of the generic streams,
  * threads = 128 (default: register-resident heat streams where they apply)
  * or 256 (always the generic shared-memory streams).
- * The defaults reproduce the reference's MPSS with bs-row bands.
+ * The defaults reproduce the reference's bs-row bands with MPSS levels per
+ * half-cycle, except heat with forward Euler at bs 32 (12 levels, measured
+ * faster); results do not depend on the tiling.
  */
 int ps_configure(ps_solver *s, int h, int nseg, int chunk, int threads);
+
+/*
+ * The tiling in use: levels per half-cycle, column blocks per band (after a
+ * swept run, the count it chose), chunk width and MPSS (bs/(2*OPS) - 1, the
+ * most levels a half-cycle can hold).  Any pointer may be NULL.  No
+ * counterpart in the reference, whose half-cycle is always MPSS levels
+ * (pysweep/core/solver.py:113-128).
+ */
+int ps_get_tiling(ps_solver *s, int *h, int *nseg, int *chunk, int *mpss);
 
 /*
  * Upload the initial condition.  src holds `levels` fields of nv*nx*ny

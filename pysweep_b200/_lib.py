@@ -50,6 +50,7 @@ _SIGS = {
                                            ctypes.POINTER(ctypes.c_double)]),
     "ps_configure": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int]),
+    "ps_get_tiling": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 4),
     "ps_set_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "ps_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
                               ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),

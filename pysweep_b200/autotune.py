@@ -86,7 +86,7 @@ def candidates(equation, nx, ny, its=1, ops=None, blocksizes=None):
         mpss = bs // (2 * ops) - 1
         if mpss < max(1, its):
             continue
-        hs = sorted({mpss, max(its, (2 * mpss) // 3)})
+        hs = sorted({mpss, max(its, (4 * mpss) // 5), max(its, (2 * mpss) // 3)})
         nb = nx // bs
         fast = register_streams(equation, ny, its, bs)
         segs = {0}  # 0 = the library's automatic choice

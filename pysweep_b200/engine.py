@@ -83,6 +83,13 @@ class Engine:
     def configure(self, h=0, nseg=0, chunk=0, threads=0):
         check(_lib.lib().ps_configure(self._h, h, nseg, chunk, threads), self._h)
 
+    def tiling(self):
+        """{"h", "nseg", "chunk", "mpss"}: levels per half-cycle, column blocks
+        per band (the count the last swept run chose), chunk width, MPSS."""
+        v = [ctypes.c_int() for _ in range(4)]
+        check(_lib.lib().ps_get_tiling(self._h, *[ctypes.byref(x) for x in v]), self._h)
+        return dict(zip(("h", "nseg", "chunk", "mpss"), (x.value for x in v)))
+
     # -- state -------------------------------------------------------------
     # Torch tensors are read and written on the solver's stream.  Unless that
     # stream is torch's current one, the solver first waits for work queued on

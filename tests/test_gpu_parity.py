@@ -217,3 +217,29 @@ def test_streaming_standard_heat_matches_generic_and_oracle(scheme, its, n):
     assert np.array_equal(fast, gen)
     assert np.array_equal(ff, gf)
     assert np.array_equal(fast, ref[: len(fast)])
+
+
+def test_default_levels_per_half_cycle_and_tiling_query():
+    """Heat with forward Euler at bs 32 runs 12 levels per half-cycle unless
+    configured (every other shape MPSS); the tiling changes no bit."""
+    from pysweep_b200 import Engine, plugin_constants
+    n, steps = 256, 53
+    ic, g = _ic_and_globals("heat", n, steps, True)
+    out = {}
+    for h in (0, 15, 9):
+        e = Engine("heat", n, n, blocksize=32)
+        for k, v in plugin_constants("heat", g).items():
+            e.set_global(k, v)
+        if h:
+            e.configure(h=h)
+        e.set_state(ic)
+        e.run(steps)
+        t = e.tiling()
+        assert t["mpss"] == 15 and t["h"] == (h or 12) and t["nseg"] >= 1
+        out[h] = e.get_state()
+        e.close()
+    ref, _, _ = oracle.standard("heat", ic, g, 1, steps)
+    for h in out:
+        assert np.array_equal(out[h], ref[-1])
+    assert Engine("heat", 64, 64, blocksize=16).tiling()["h"] == 7
+    assert Engine("euler", 64, 64, its=2, blocksize=32).tiling()["h"] == 7
