@@ -151,13 +151,14 @@ def fp64_roof(cells, ms, clk):
             "peak_ginstr_s": peak, "frac": achieved / peak, "sm_mhz": mhz}
 
 
-def ncu_traffic(kind, n, bs):
-    """DRAM bytes per launch of one kernel kind, from a committed ncu summary."""
+def ncu_traffic(kind, n, bs, h):
+    """DRAM bytes per launch of one kernel kind (h levels per half-cycle),
+    from a committed ncu summary."""
     p = os.path.join(ROOT, "profiles", f"heat2d_swept_{kind}_traffic.txt")
     try:
         for line in open(p):
             k, _, v = line.partition("=")
-            if k.strip() == f"bytes_per_launch_n{n}_bs{bs}":
+            if k.strip() == f"bytes_per_launch_n{n}_bs{bs}_h{h}":
                 return float(v)
     except OSError:
         pass
@@ -322,7 +323,7 @@ def run_b200(args):
     dms, dn, dcells = kinds[dom]
     achieved = dcells * cell_bytes / (dms / 1000) / 1e9
     peak, peak_src = measured_peak()
-    traffic = None if f32 else ncu_traffic(dom, n, bs)
+    traffic = None if f32 else ncu_traffic(dom, n, bs, eng.tiling()["h"])
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "kernel": dom,
             "launches": dn, "avg_launch_ms": dms / dn,
