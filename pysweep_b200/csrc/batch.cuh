@@ -14,10 +14,14 @@
 
 namespace psb {
 
+// Descriptors [instance][role][parity]: role 0 for the prism stream and the
+// y-bridge, role 1 for the gap stream and the octahedron (their y-faces live in
+// a second buffer, because the gap runs beside the y-bridge).
+template <bool GAP>
 __device__ __forceinline__ void batch_args(const SweptArgs* __restrict__ desc, int inst,
                                            int parity, int H, long long L0, SweptArgs& a)
 {
-    a = desc[2 * inst + parity];
+    a = desc[4 * inst + 2 * (GAP ? 1 : 0) + parity];
     a.H = H;
     a.L0 = L0;
 }
@@ -33,7 +37,7 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3)
     if (g >= nunits) return;  // whole warp
     const int2 u = units[g];
     SweptArgs a;
-    batch_args(desc, u.x, parity, H, L0, a);
+    batch_args<GAP>(desc, u.x, parity, H, L0, a);
     heat_fast_body<BX, GAP>(a, u.y, sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
@@ -49,7 +53,7 @@ __global__ void __launch_bounds__(NT, 2)
     extern __shared__ double sm[];
     const int2 u = units[blockIdx.x];
     SweptArgs a;
-    batch_args(desc, u.x, parity, H, L0, a);
+    batch_args<GAP>(desc, u.x, parity, H, L0, a);
     stream_body<Eq, ITS, W, GAP, NT>(a, u.y, sm);
 }
 
@@ -61,7 +65,7 @@ __global__ void __launch_bounds__(NT, 4)
     extern __shared__ double sm[];
     const int2 u = units[blockIdx.x];
     SweptArgs a;
-    batch_args(desc, u.x, parity, H, L0, a);
+    batch_args<GAP>(desc, u.x, parity, H, L0, a);
     seam_body<Eq, ITS, GAP, NT>(a, u.y, sm);
 }
 

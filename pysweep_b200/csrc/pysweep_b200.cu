@@ -1043,6 +1043,7 @@ struct BatchInst {
     double* base[2] = {nullptr, nullptr};
     double* xface = nullptr;
     double* yface = nullptr;
+    size_t yface_n = 0;  // elements of both y-face buffers
     bool have_state = false;
     std::map<std::string, double> globals;
 };
@@ -1053,8 +1054,11 @@ struct ps_batch {
     bool fast = false;
     bool faces = false;  // Euler streams share faces (scratch beside the tile)
     cudaStream_t stream = nullptr;
+    // the gap stream runs beside the y-bridge on a high-priority side stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<BatchInst> inst;
-    SweptArgs* d_desc = nullptr;  // [2 * count]: even / odd half-cycles
+    SweptArgs* d_desc = nullptr;  // [count][2 roles][2 parities] (batch_args)
     int2* d_units = nullptr;      // (instance, unit) of every band segment
     int nunits = 0;
     int cur = 0;                  // base holding the current levels (all instances)
@@ -1109,17 +1113,18 @@ void batch_free_graph(ps_batch* b)
 int batch_upload(ps_batch* b)
 {
     const int n = (int)b->inst.size();
-    std::vector<SweptArgs> d(2 * n);
+    std::vector<SweptArgs> d(4 * n);
     const int O2 = 2 * b->ops;
     for (int i = 0; i < n; ++i) {
         const BatchInst& I = b->inst[i];
-        for (int par = 0; par < 2; ++par) {
-            SweptArgs& a = d[2 * i + par];
+        for (int q = 0; q < 4; ++q) {
+            const int role = q / 2, par = q % 2;
+            SweptArgs& a = d[4 * i + q];
             memset(&a, 0, sizeof a);
             a.bin = I.base[par];
             a.bout = I.base[1 - par];
             a.xface = I.xface;
-            a.yface = I.yface;
+            a.yface = I.yface + (role ? I.yface_n / 2 : 0);
             a.frame_every = 1;
             a.nx = I.nx;
             a.ny = I.ny;
@@ -1176,29 +1181,40 @@ struct BatchKernels {
     const void* O = nullptr;
 };
 
-// Enqueue one half-cycle for every instance.
+// Enqueue one half-cycle for every instance: P, then Y on the batch stream
+// beside G on the side stream (G reads nothing Y writes; see run_swept), then
+// O after both.
 template <class Eq, int ITS, int W>
 void batch_half(ps_batch* b, int par, int H, long long L0, size_t ssm, size_t gsm, dim3 fgrid)
 {
     const int nu = b->nunits;
+    cudaStream_t st = b->stream, sd = b->side;
+    auto fork = [&] {
+        cudaEventRecord(b->ev_fork, st);
+        cudaStreamWaitEvent(sd, b->ev_fork, 0);
+    };
+    auto join = [&] {
+        cudaEventRecord(b->ev_join, sd);
+        cudaStreamWaitEvent(st, b->ev_join, 0);
+    };
     if (b->fast) {
         if (b->bs == 16) {
-            heat_stream_fast_batch<16, false><<<fgrid, 32 * kFastWarps, gsm, b->stream>>>(b->d_desc, b->d_units, nu, par, H, L0);
-            seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
-            heat_stream_fast_batch<16, true><<<fgrid, 32 * kFastWarps, gsm, b->stream>>>(b->d_desc, b->d_units, nu, par, H, L0);
-            seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+            heat_stream_fast_batch<16, false><<<fgrid, 32 * kFastWarps, gsm, st>>>(b->d_desc, b->d_units, nu, par, H, L0);
+            fork();
+            heat_stream_fast_batch<16, true><<<fgrid, 32 * kFastWarps, gsm, sd>>>(b->d_desc, b->d_units, nu, par, H, L0);
         } else {
-            heat_stream_fast_batch<32, false><<<fgrid, 32 * kFastWarps, gsm, b->stream>>>(b->d_desc, b->d_units, nu, par, H, L0);
-            seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
-            heat_stream_fast_batch<32, true><<<fgrid, 32 * kFastWarps, gsm, b->stream>>>(b->d_desc, b->d_units, nu, par, H, L0);
-            seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+            heat_stream_fast_batch<32, false><<<fgrid, 32 * kFastWarps, gsm, st>>>(b->d_desc, b->d_units, nu, par, H, L0);
+            fork();
+            heat_stream_fast_batch<32, true><<<fgrid, 32 * kFastWarps, gsm, sd>>>(b->d_desc, b->d_units, nu, par, H, L0);
         }
     } else {
-        stream_batch<Eq, ITS, W, false, 256><<<nu, 256, gsm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
-        seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
-        stream_batch<Eq, ITS, W, true, 256><<<nu, 256, gsm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
-        seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, b->stream>>>(b->d_desc, b->d_units, par, H, L0);
+        stream_batch<Eq, ITS, W, false, 256><<<nu, 256, gsm, st>>>(b->d_desc, b->d_units, par, H, L0);
+        fork();
+        stream_batch<Eq, ITS, W, true, 256><<<nu, 256, gsm, sd>>>(b->d_desc, b->d_units, par, H, L0);
     }
+    seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, st>>>(b->d_desc, b->d_units, par, H, L0);
+    join();
+    seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, st>>>(b->d_desc, b->d_units, par, H, L0);
 }
 
 template <class Eq, int ITS, int W>
@@ -1338,6 +1354,11 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
     if (rc == PS_OK) {
         cudaError_t e = cudaSetDevice(device);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        int lo = 0, hi = 0;
+        if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, hi);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
         if (e != cudaSuccess) rc = bfail(b, PS_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
     }
     const int O2 = 2 * ops, HF = b->H - 1;
@@ -1345,7 +1366,9 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
         if (rc != PS_OK) break;
         const size_t f = (size_t)nv * I.nx * I.ny;
         const size_t xn = (size_t)I.nb * HF * 2 * nv * O2 * I.ny;
-        const size_t yn = (size_t)I.nb * I.nseg * 2 * HF * nv * blocksize * O2;
+        // two y-face buffers: prism -> y-bridge and gap -> octahedron
+        const size_t yn = 2 * (size_t)I.nb * I.nseg * 2 * HF * nv * blocksize * O2;
+        I.yface_n = yn;
         cudaError_t e = cudaMalloc(&I.base[0], f * its * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&I.base[1], f * its * sizeof(double));
         if (e == cudaSuccess && xn) e = cudaMalloc(&I.xface, xn * sizeof(double));
@@ -1354,7 +1377,7 @@ int ps_batch_create(ps_batch** out, int device, int equation, int count, const i
     }
     if (rc == PS_OK) {
         b->nunits = (int)units.size();
-        cudaError_t e = cudaMalloc(&b->d_desc, 2 * b->inst.size() * sizeof(SweptArgs));
+        cudaError_t e = cudaMalloc(&b->d_desc, 4 * b->inst.size() * sizeof(SweptArgs));
         if (e == cudaSuccess) e = cudaMalloc(&b->d_units, units.size() * sizeof(int2));
         if (e == cudaSuccess)
             e = cudaMemcpy(b->d_units, units.data(), units.size() * sizeof(int2), cudaMemcpyHostToDevice);
@@ -1388,6 +1411,12 @@ int ps_batch_destroy(ps_batch* b)
     }
     if (b->d_desc) cudaFree(b->d_desc);
     if (b->d_units) cudaFree(b->d_units);
+    if (b->side) {
+        cudaStreamSynchronize(b->side);
+        cudaStreamDestroy(b->side);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return PS_OK;
