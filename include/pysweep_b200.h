@@ -192,9 +192,9 @@ const char *ps_last_error(const ps_solver *s);
 /*
  * Swept heat solve (forward Euler, the heat plugin's arithmetic) that
  * allocates nothing.  No counterpart in the reference: it exists for callers
- * that cannot call cudaMalloc at the time they solve -- code running inside
- * someone else's CUDA graph capture, a process whose memory pool owns the
- * device, a real-time loop that must not touch the allocator.  The caller
+ * that cannot call cudaMalloc at the time they solve -- a process whose memory
+ * pool already owns the device memory, a real-time loop that must not touch
+ * the allocator.  The caller
  * passes the input and output fields (device pointers, nx*ny doubles, distinct);
  * every temporary lives in one static device array of 128 MiB that each GPU
  * holds from library load to process exit.  Sizes whose scratch (one field plus

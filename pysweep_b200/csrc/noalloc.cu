@@ -2,8 +2,7 @@
 // device memory.
 //
 // Some hosts of this library run where a cudaMalloc is not allowed at call
-// time: code executing inside a captured CUDA graph region of someone else's
-// framework, plugins of a process whose memory pool owns the whole device, or
+// time: plugins of a process whose memory pool owns the whole device, or
 // real-time loops that must not touch the allocator.  This entry point takes
 // only the caller's input and output fields and keeps every temporary buffer
 // in one file-scope device array, g_noalloc_scratch, that the CUDA runtime

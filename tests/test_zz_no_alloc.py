@@ -1,8 +1,8 @@
 """ps_heat_swept_noalloc, the entry point for callers that cannot allocate.
 
-Callers inside another framework's graph capture or under a foreign memory
-pool cannot cudaMalloc when they solve; this entry point keeps its scratch in a
-static device array instead.  It must give exactly what the allocating path
+Callers under a foreign memory pool that owns the device, or in loops that
+must not touch the allocator, cannot cudaMalloc when they solve; this entry
+point keeps its scratch in a static device array instead.  It must give exactly what the allocating path
 (ps_run on a ps_solver) gives, on consecutive calls that share the array.
 This file is collected last on purpose.
 """
