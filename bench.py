@@ -172,11 +172,29 @@ def cpu_baseline(n_sample, bs, levels_cycles, threads):
     g = heat_globals(n_sample, 10)
     mpss = bs // 2 - 1
     t0 = time.perf_counter()
-    oracle.swept("heat", ic, g, 1, 1, bs, max_gss=levels_cycles - 1, nthreads=threads,
-                  frames=False)
+    _, fin = oracle.swept("heat", ic, g, 1, 1, bs, max_gss=levels_cycles - 1, nthreads=threads,
+                          frames=False)
     dt = time.perf_counter() - t0
     cells = float(n_sample) ** 2 * mpss * levels_cycles
-    return cells / dt / 1e9, dt
+    return cells / dt / 1e9, dt, (ic, g, mpss * levels_cycles, fin)
+
+
+def parity_check(sample, bs, device):
+    """The GPU path on the CPU baseline's own sample, checked against the
+    oracle's result of that run (max relative error, bitwise equality)."""
+    from pysweep_b200 import Engine, plugin_constants
+    ic, g, nlev, fin = sample
+    n = ic.shape[-1]
+    e = Engine("heat", n, n, blocksize=bs, device=device)
+    for k, v in plugin_constants("heat", g).items():
+        e.set_global(k, v)
+    e.set_state(ic)
+    e.run(nlev)
+    got = e.get_state()
+    e.close()
+    err = float(np.max(np.abs(got - fin)) / max(np.max(np.abs(fin)), 1e-300))
+    return {"sample": f"{n}x{n} heat, bs {bs}, {nlev} levels (the cpu_baseline run)",
+            "max_rel_err_vs_oracle": err, "bitwise_equal": bool(np.array_equal(got, fin))}
 
 
 def run_reference(args):
@@ -186,7 +204,7 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     vals = []
     for i in range(args.warmup + args.steps):
-        v, _ = cpu_baseline(args.ref_n, args.bs, args.ref_cycles, threads)
+        v, _, _ = cpu_baseline(args.ref_n, args.bs, args.ref_cycles, threads)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
@@ -345,11 +363,12 @@ def run_b200(args):
             "tiling": dict(eng.tiling(), nseg_auto=not args.nseg)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not f32:
         threads = os.cpu_count() or 1
-        v, secs = cpu_baseline(args.ref_n, bs, args.ref_cycles, threads)
+        v, secs, sample = cpu_baseline(args.ref_n, bs, args.ref_cycles, threads)
         line["cpu_baseline"] = {
             "value": v, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{args.ref_n}x{args.ref_n} heat, bs {bs}, {args.ref_cycles} swept "
                       f"half-cycles, {secs:.1f} s"}
+        line["parity"] = parity_check(sample, bs, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
