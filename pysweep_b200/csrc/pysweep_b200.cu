@@ -405,6 +405,8 @@ size_t stream_smem(const ps_solver* s)
 
 size_t seam_smem(const ps_solver* s)
 {
+    if (seam_direct(s->bs, s->ops, s->nv, s->its, s->H, s->esize))
+        return s->esize * (size_t)(s->its + 1) * s->nv * s->bs * (2 * s->ops * (s->H + 1));
     return s->esize * std::max(seam_smem_elems(false, s->bs, s->ops, s->nv, s->its, s->H),
                                seam_smem_elems(true, s->bs, s->ops, s->nv, s->its, s->H));
 }
@@ -515,6 +517,7 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     a.xface = s->xface;
     a.yface = s->yface;
     a.p = make_params(s);
+    a.seam_direct = seam_direct(s->bs, s->ops, s->nv, s->its, s->H, s->esize) ? 1 : 0;
     const int units = a.nb * a.nseg;
     const size_t fe = field_elems(s);
     int off = 0;
@@ -1142,6 +1145,7 @@ int batch_upload(ps_batch* b)
             a.its = b->its;
             a.gts_base = 0;
             a.p = make_params_g(b->eq, I.globals);
+            a.seam_direct = seam_direct(b->bs, b->ops, b->nv, b->its, b->H, sizeof(double)) ? 1 : 0;
         }
         (void)O2;
     }
@@ -1167,6 +1171,8 @@ size_t batch_stream_smem(const ps_batch* b)
 
 size_t batch_seam_smem(const ps_batch* b)
 {
+    if (seam_direct(b->bs, b->ops, b->nv, b->its, b->H, sizeof(double)))
+        return sizeof(double) * (size_t)(b->its + 1) * b->nv * b->bs * (2 * b->ops * (b->H + 1));
     return sizeof(double) * std::max(seam_smem_elems(false, b->bs, b->ops, b->nv, b->its, b->H),
                                      seam_smem_elems(true, b->bs, b->ops, b->nv, b->its, b->H));
 }

@@ -62,6 +62,9 @@ struct SweptArgs {
     int seg_unit, seg_units;
     int off;      // first row of prism band 0 (prism bands: off + i*bx)
     int its;
+    // 1: the seams read each level's faces from HBM when they reach it
+    // instead of staging all of them in shared memory first (seam_direct)
+    int seam_direct;
     long long L0;  // global level index of this half-cycle's level 0
     int gts_base;  // the step function sees globalTimeStep = gts_base + level
     EqParams p;
@@ -160,6 +163,20 @@ __host__ __device__ inline size_t seam_smem_elems(bool gap, int bx, int ops, int
 {
     const size_t slots = (size_t)(its + 1) * nv * bx * (2 * ops * (hmax + 1));
     return slots + seam_yoff(gap, bx, ops, nv, hmax) + (gap ? seam_xoff(ops, nv, hmax) : 0);
+}
+
+// Whether the seams skip the staging: where the staged faces would leave
+// two or fewer seam CTAs per SM and the bare tile slots fit more (large
+// Euler tiles; heat tiles keep seven with staging).
+__host__ __device__ inline bool seam_direct(int bx, int ops, int nv, int its, int hmax,
+                                            size_t esize)
+{
+    const size_t cap = 227 * 1024;
+    const size_t ys = seam_smem_elems(false, bx, ops, nv, its, hmax);
+    const size_t gs = seam_smem_elems(true, bx, ops, nv, its, hmax);
+    const size_t staged = esize * (ys > gs ? ys : gs);
+    const size_t bare = esize * (size_t)(its + 1) * nv * bx * (2 * ops * (hmax + 1));
+    return cap / staged <= 2 && cap / bare > cap / staged;
 }
 
 // Frame slot for global level L, or -1.
@@ -464,7 +481,8 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
     // edge) and, in the gap, the prisms' rows around it [v][rr][column]
     T* ystage = slot + NSLOT * SL;
     T* xstage = ystage + seam_yoff(GAP, BX, OPS, nv, a.Hmax);
-    for (int m = 1; m <= H - 1; ++m) {
+    const bool direct = a.seam_direct != 0;
+    for (int m = 1; m <= (direct ? 0 : H - 1); ++m) {
         const int rlo = GAP ? hx - OPS * m : OPS * m;
         const int nr = seam_rows(GAP, BX, OPS, m), n = nv * nr * O2;
         const T* yl = yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
@@ -514,12 +532,15 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
             // right part from the right block's left edge.
             const int n = nv * nr * O2;
             const T* ys = ystage + seam_yoff(GAP, BX, OPS, nv, m);
+            const T* yl = yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
+            const T* yr = yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
             for (int v = 0; v < nv; ++v)
                 for_2d<NT>(nr, O2, tid, [&](int r, int j) {
                     const int e = (v * nr + r) * O2 + j;
+                    const int src = (v * BX + rlo + r) * O2 + j;
                     T* row = out + (v * BX + rlo + r) * TW;
-                    row[clo - O2 + j] = ys[e];
-                    row[chi + j] = ys[n + e];
+                    row[clo - O2 + j] = direct ? yl[src] : ys[e];
+                    row[chi + j] = direct ? yr[src] : ys[n + e];
                 });
             if (GAP) {
                 // the prisms' rows around the gap, columns [clo-2OPS, chi+2OPS)
@@ -529,7 +550,17 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
                     for_2d<NT>(2 * O2, nc2, tid, [&](int rr, int kk) {
                         const int j = rr < O2 ? rr : rr - O2;
                         const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
-                        out[(v * BX + i) * TW + clo - O2 + kk] = xs[(v * 2 * O2 + rr) * nc2 + kk];
+                        T val;
+                        if (direct) {
+                            const int side = rr < O2 ? 1 : 0;
+                            const int bb = rr < O2 ? bup : band;
+                            const size_t fo =
+                                ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                            val = xface[fo * ny + xface_col(gcol(clo - O2 + kk), m, ny)];
+                        } else {
+                            val = xs[(v * 2 * O2 + rr) * nc2 + kk];
+                        }
+                        out[(v * BX + i) * TW + clo - O2 + kk] = val;
                     });
             }
         }
