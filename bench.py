@@ -4,7 +4,8 @@
 Workload (one "step" = one full solve): the 2-D heat equation u_t = u_xx + u_yy
 on the periodic unit square, 8192 x 8192 FP64 cells, forward Euler with
 dt = 0.2*dx^2, 5000 time steps, swept decomposition with blocksize 32
-(15 levels per half-cycle).  The initial field is a seeded sum of 8 periodic
+(12 levels per half-cycle, the library's default for this shape; at most
+15 fit a 32-row band).  The initial field is a seeded sum of 8 periodic
 Fourier modes (amplitudes U(0,1)).  The 537 MB field is larger than the
 126 MB L2, so consecutive steps do not run from cache.
 
