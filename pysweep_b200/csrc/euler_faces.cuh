@@ -5,6 +5,7 @@
 // euler::dface, euler::update), so the results are bitwise equal.
 #pragma once
 #include "equations.cuh"
+#include "swept.cuh"
 
 namespace psb {
 
@@ -90,11 +91,15 @@ __global__ void __launch_bounds__(kEuNT, 2)
     const int tid = threadIdx.x;
     const size_t plane = (size_t)nx * ny;
     const double dtdx = p.d[0], dtdy = p.d[1], gamma = p.d[2], gm1 = p.d[3];
+    // the tile and its halo arrive by cp.async: every copy of a thread is in
+    // flight at once
     for (int e = tid; e < 4 * kEuHRC; e += kEuNT) {
         const int c = e % kEuHC, r = (e / kEuHC) % kEuHR, v = e / kEuHRC;
         const int x = eu_wrap(x0 + r - 2, nx), y = eu_wrap(y0 + c - 2, ny);
-        q[e] = cur[v * plane + (size_t)x * ny + y];
+        cp_async8(q + e, cur + v * plane + (size_t)x * ny + y);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     for (int e = tid; e < kEuHRC; e += kEuNT)
         P[e] = euler::pressure(gm1, q[e], q[e + kEuHRC], q[e + 2 * kEuHRC], q[e + 3 * kEuHRC]);
