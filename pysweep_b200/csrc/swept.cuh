@@ -238,11 +238,13 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
             double* s0p = slot;  // slot of level 0
             const double* b0 = a.bin + (size_t)(ITS - 1) * nv * nx * ny;
             const int n0 = nv * (hi0 - lo0) * RC;
+            // level 0 (and level -1) arrive by cp.async: every copy of a
+            // thread is in flight at once
             for (int e = tid; e < n0; e += NT) {
                 const int k = e % RC, t = e / RC;
                 const int i = lo0 + t % (hi0 - lo0), v = t / (hi0 - lo0);
                 const int g = wrap(cw - O2 + k, ny), r = wrap(r0 + i, nx);
-                s0p[(v * BX + i) * RS + k] = b0[((size_t)v * nx + r) * ny + g];
+                cp_async8(s0p + (v * BX + i) * RS + k, b0 + ((size_t)v * nx + r) * ny + g);
             }
             if (ITS >= 2) {
                 const int lo1 = GAP ? hx - OPS : OPS, hi1 = GAP ? hx + OPS : BX - OPS;
@@ -253,9 +255,11 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
                     const int k = e % Wc, t = e / Wc;
                     const int i = lo1 + t % (hi1 - lo1), v = t / (hi1 - lo1);
                     const int g = wrap(cw - OPS + k, ny), r = wrap(r0 + i, nx);
-                    s1p[(v * BX + i) * RS + k] = b1[((size_t)v * nx + r) * ny + g];
+                    cp_async8(s1p + (v * BX + i) * RS + k, b1 + ((size_t)v * nx + r) * ny + g);
                 }
             }
+            cp_async_commit();
+            cp_async_wait<0>();
         }
         __syncthreads();
 
@@ -463,7 +467,8 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
         for (int v = 0; v < nv; ++v)
             for_2d<NT>(hi0 - lo0, 2 * O2, tid, [&](int r, int c) {
                 const int i = lo0 + r, k = KC - O2 + c;
-                slot[(v * BX + i) * TW + k] = b0[((size_t)v * nx + grow(i)) * ny + gcol(k)];
+                cp_async_elem(slot + (v * BX + i) * TW + k,
+                              b0 + ((size_t)v * nx + grow(i)) * ny + gcol(k));
             });
         if (ITS >= 2) {
             const int lo1 = GAP ? hx - OPS : OPS, hi1 = GAP ? hx + OPS : BX - OPS;
@@ -472,7 +477,8 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
             for (int v = 0; v < nv; ++v)
                 for_2d<NT>(hi1 - lo1, O2, tid, [&](int r, int c) {
                     const int i = lo1 + r, k = KC - OPS + c;
-                    s1p[(v * BX + i) * TW + k] = b1[((size_t)v * nx + grow(i)) * ny + gcol(k)];
+                    cp_async_elem(s1p + (v * BX + i) * TW + k,
+                                  b1 + ((size_t)v * nx + grow(i)) * ny + gcol(k));
                 });
         }
     }
