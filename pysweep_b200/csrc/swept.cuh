@@ -271,6 +271,27 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
             const double* cur = slot + ((m - 1) % NSLOT) * SL;
             const double* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
             const int gts = a.gts_base + (int)(a.L0 + m);
+            // gap: the prisms' rows of level m that the next level reads go
+            // into level m's slot by cp.async while the level is computed
+            // (rows outside the level's own, a slot no level still reads)
+            if (GAP && m <= H - 1) {
+                const int nrow = 2 * O2;  // top band's bottom face + bottom band's top face
+                const int n = nv * nrow * Wc;
+                const int bup = wrap(band - 1, a.nb), bdn = band;
+                for (int e = tid; e < n; e += NT) {
+                    const int k = O2 + e % Wc, t = e / Wc;
+                    const int rr = t % nrow, v = t / nrow;
+                    const int side = rr < O2 ? 1 : 0;      // 1 = bottom face of upper band
+                    const int j = rr < O2 ? rr : rr - O2;
+                    const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
+                    const int bb = rr < O2 ? bup : bdn;
+                    const int g = wrap(cw - OPS * m - O2 + k, ny);
+                    const size_t fo =
+                        ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                    cp_async8(out + (v * BX + i) * RS + k, a.xface + fo * ny + xface_col(g, m, ny));
+                }
+                cp_async_commit();
+            }
             // compute level m
             if constexpr (FaceLevel<Eq>::value) {
                 // faces shared between the cells of the level (scratch after the carry)
@@ -302,24 +323,7 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
                     cout_[e] = cur[t * RS + W + j];
                 }
             }
-            // gap: the prisms' rows of level m that the next level reads
-            if (GAP && m <= H - 1) {
-                const int nrow = 2 * O2;  // top band's bottom face + bottom band's top face
-                const int n = nv * nrow * Wc;
-                const int bup = wrap(band - 1, a.nb), bdn = band;
-                for (int e = tid; e < n; e += NT) {
-                    const int k = O2 + e % Wc, t = e / Wc;
-                    const int rr = t % nrow, v = t / nrow;
-                    const int side = rr < O2 ? 1 : 0;      // 1 = bottom face of upper band
-                    const int j = rr < O2 ? rr : rr - O2;
-                    const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
-                    const int bb = rr < O2 ? bup : bdn;
-                    const int g = wrap(cw - OPS * m - O2 + k, ny);
-                    const size_t fo =
-                        ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                    out[(v * BX + i) * RS + k] = a.xface[fo * ny + xface_col(g, m, ny)];
-                }
-            }
+            if (GAP) cp_async_wait<0>();  // the face rows issued before the compute
             __syncthreads();
             // ---- outputs of level m --------------------------------------
             {
@@ -529,47 +533,64 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
         const T* cur = slot + ((m - 1) % NSLOT) * SL;
         const T* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
         const int gts = a.gts_base + (int)(a.L0 + m);
+        // level m's faces go to cells of level m's slot that the level does
+        // not compute (columns beside the bridge, rows around the gap), and
+        // the slot's previous level is no longer read: unstaged, they are
+        // copied by cp.async while the level is computed; staged, afterwards
+        // from shared memory
+        const int n = nv * nr * O2, nc2 = nc + 2 * O2;
+        const T* yl = yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
+        const T* yr = yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
+        if (direct && m <= H - 1) {
+            for (int v = 0; v < nv; ++v)
+                for_2d<NT>(nr, O2, tid, [&](int r, int j) {
+                    const int src = (v * BX + rlo + r) * O2 + j;
+                    T* row = out + (v * BX + rlo + r) * TW;
+                    cp_async_elem(row + clo - O2 + j, yl + src);
+                    cp_async_elem(row + chi + j, yr + src);
+                });
+            if (GAP) {
+                for (int v = 0; v < nv; ++v)
+                    for_2d<NT>(2 * O2, nc2, tid, [&](int rr, int kk) {
+                        const int j = rr < O2 ? rr : rr - O2;
+                        const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
+                        const int side = rr < O2 ? 1 : 0;
+                        const int bb = rr < O2 ? bup : band;
+                        const size_t fo =
+                            ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
+                        cp_async_elem(out + (v * BX + i) * TW + clo - O2 + kk,
+                                      xface + fo * ny + xface_col(gcol(clo - O2 + kk), m, ny));
+                    });
+            }
+            cp_async_commit();
+        }
         for_2d<NT>(nr, nc, tid, [&](int r, int c) {
             const int o = (rlo + r) * TW + clo + c;
             Eq::step(cur + o, prv + o, out + o, nb, gts, nv, a.p);
         });
-        if (m <= H - 1) {
+        if (!direct && m <= H - 1) {
             // y-faces of level m: left part from the left block's right edge,
             // right part from the right block's left edge.
-            const int n = nv * nr * O2;
             const T* ys = ystage + seam_yoff(GAP, BX, OPS, nv, m);
-            const T* yl = yface + ((((size_t)ul * 2 + 1) * HF + (m - 1)) * nv) * BX * O2;
-            const T* yr = yface + ((((size_t)ur * 2 + 0) * HF + (m - 1)) * nv) * BX * O2;
             for (int v = 0; v < nv; ++v)
                 for_2d<NT>(nr, O2, tid, [&](int r, int j) {
                     const int e = (v * nr + r) * O2 + j;
-                    const int src = (v * BX + rlo + r) * O2 + j;
                     T* row = out + (v * BX + rlo + r) * TW;
-                    row[clo - O2 + j] = direct ? yl[src] : ys[e];
-                    row[chi + j] = direct ? yr[src] : ys[n + e];
+                    row[clo - O2 + j] = ys[e];
+                    row[chi + j] = ys[n + e];
                 });
             if (GAP) {
                 // the prisms' rows around the gap, columns [clo-2OPS, chi+2OPS)
-                const int nc2 = nc + 2 * O2;
                 const T* xs = xstage + seam_xoff(OPS, nv, m);
                 for (int v = 0; v < nv; ++v)
                     for_2d<NT>(2 * O2, nc2, tid, [&](int rr, int kk) {
                         const int j = rr < O2 ? rr : rr - O2;
                         const int i = rr < O2 ? hx - OPS * m - O2 + j : hx + OPS * m + j;
-                        T val;
-                        if (direct) {
-                            const int side = rr < O2 ? 1 : 0;
-                            const int bb = rr < O2 ? bup : band;
-                            const size_t fo =
-                                ((((size_t)bb * HF + (m - 1)) * 2 + side) * nv + v) * O2 + j;
-                            val = xface[fo * ny + xface_col(gcol(clo - O2 + kk), m, ny)];
-                        } else {
-                            val = xs[(v * 2 * O2 + rr) * nc2 + kk];
-                        }
-                        out[(v * BX + i) * TW + clo - O2 + kk] = val;
+                        out[(v * BX + i) * TW + clo - O2 + kk] = xs[(v * 2 * O2 + rr) * nc2 + kk];
                     });
             }
         }
+        if (direct) cp_async_wait<0>();
         __syncthreads();
         // outputs of level m
         if (!GAP && m <= H - 1) {
