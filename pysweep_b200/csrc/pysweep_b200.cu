@@ -472,16 +472,15 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
             s->nseg = std::max(1, std::min(s->ny / kFastChunk, slots / nb));
             s->nseg = std::max(1, std::min(s->nseg, s->ny / 32));
         } else {
-            // one CTA per (band, segment): the most segments up to about four
-            // CTAs per SM, each dividing ny and at least one chunk and
-            // 2*ops*(h+1) columns wide (narrower segments add seam work)
-            int sms = 148;
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-            const int nb = s->nx / s->bs;
-            const int want = std::max(1, (4 * sms + nb - 1) / nb);
-            const int minw = std::max(s->chunk, O2 * (s->H + 1));
+            // one CTA per (band, segment): the most segments that divide ny
+            // and keep four chunks (and 2*ops*(h+1) columns) each.  Shorter
+            // segments make the seams as costly as the streams; longer ones
+            // leave few, long CTAs and a ragged last wave.  Measured on Euler
+            // (G cell-stages/s): 1024², bs 32: 16 segments 3.00, 8: 3.31,
+            // 4: 3.32; 4096², bs 16: 2: 5.65, 16: 6.26, 32: 5.93, 64: 5.39.
+            const int minw = std::max(4 * s->chunk, O2 * (s->H + 1));
             s->nseg = 1;
-            for (int q = 2; q <= want && s->ny / q >= minw; ++q)
+            for (int q = 2; s->ny / q >= minw; ++q)
                 if (s->ny % q == 0) s->nseg = q;
         }
     }
