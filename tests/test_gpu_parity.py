@@ -243,3 +243,22 @@ def test_default_levels_per_half_cycle_and_tiling_query():
         assert np.array_equal(out[h], ref[-1])
     assert Engine("heat", 64, 64, blocksize=16).tiling()["h"] == 7
     assert Engine("euler", 64, 64, its=2, blocksize=32).tiling()["h"] == 7
+
+
+def test_generic_streams_choose_segments_of_four_chunks():
+    """The shared-memory streams cut each band into the most segments that
+    divide the row and keep four chunks each (1024 columns in 32-column
+    chunks, the widest whose bs-32 Euler tile fits: 8 segments), chosen at
+    the first swept run."""
+    from pysweep_b200 import Engine, plugin_constants
+    from pysweep_b200.equations.euler import analytical_array
+    n = 1024
+    dx = 10.0 / n
+    e = Engine("euler", n, n, its=2, blocksize=32)
+    for k, v in plugin_constants("euler", [0.0, 1.0, 0.1 * dx, dx, dx, 1.4]).items():
+        e.set_global(k, v)
+    e.set_state(analytical_array(n, n, 0.0))
+    e.run(2)
+    t = e.tiling()
+    assert t["chunk"] == 32 and t["nseg"] == n // (4 * t["chunk"])
+    e.close()
