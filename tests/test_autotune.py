@@ -31,3 +31,12 @@ def test_cached_result_is_returned_without_timing(tmp_path, monkeypatch):
         raise AssertionError("timed a tiling although the cache had the shape")
     monkeypatch.setattr(autotune, "_time_config", no_timing)
     assert autotune.tune("heat", 512, 512) == best
+
+
+def test_levels_candidates_include_four_fifths_of_mpss():
+    """Heat at bs 32 (MPSS 15) is timed at 15, 12 and 10 levels per
+    half-cycle; 12 is the library's own default for that shape."""
+    hs = {h for bs, h, _ in autotune.candidates("heat", 512, 512) if bs == 32}
+    assert hs == {15, 12, 10}
+    hs16 = {h for bs, h, _ in autotune.candidates("heat", 512, 512) if bs == 16}
+    assert hs16 == {7, 5, 4}
