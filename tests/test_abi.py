@@ -44,3 +44,13 @@ def test_plugin_constants_follow_set_globals():
     assert c == {"DT": 0.1, "DX": 0.5, "DY": 0.5, "ALPHA": 2.0, "SCHEME": True}
     c = plugin_constants("euler", [0, 1, 0.1, 0.5, 0.25, 1.4])
     assert c["GAM_M1"] == 1.4 - 1 and c["DTDX"] == 0.1 / 0.5 and c["DTDY"] == 0.1 / 0.25
+
+
+def test_package_exports_the_documented_names():
+    """The names INTEGRATION.md uses are importable from the package."""
+    import pysweep_b200
+    for name in ("Solver", "Engine", "Batch", "plugin_constants", "PySweepError"):
+        assert hasattr(pysweep_b200, name), name
+    from pysweep_b200.adjoint import heat_solve  # noqa: F401
+    from pysweep_b200.autotune import tune  # noqa: F401
+    from pysweep_b200.distributed import SlabSolver  # noqa: F401
