@@ -14,11 +14,17 @@ Reported on one JSON line (rank 0):
   standard   the same workload through the standard (one step per launch) path
   e2e        the same metric through the public API with host buffers: pinned
              host -> device upload, the run, device -> host download
-  roofline   the dominant kernel's effective bandwidth (16 B per cell update:
-             read and write of one FP64 value) against the measured HBM copy
-             bandwidth; above 1.0 means temporal reuse
+  swept_equals_standard  whether the two decompositions' 8192^2 results of
+             the timed solves are bitwise equal
+  roofline   the dominant kernel against its binding resource, the FP64 pipe
+             (FP64 instructions/s against 64 lanes per SM at the maximum SM
+             clock); its effective bandwidth (16 B per cell update: read and
+             write of one FP64 value) against the measured HBM copy bandwidth,
+             above 1.0 by the temporal reuse; and the DRAM bytes per launch
+             that ncu measured at this size
   cpu_baseline  the reference's CPU swept algorithm (C restatement) on the
              host cores, on a bounded sample of the same workload
+  secondary  the Euler, adjoint and batched targets (see secondary_lines)
 
 Under torchrun with N > 1 ranks the grid is N*8192 x 8192, one 8192-row slab
 per GPU (weak scaling), halo strips exchanged with NCCL after every swept
@@ -135,26 +141,47 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+SECONDARY_EULER_BATCH_STEPS = 100
 FP64_OPS_PER_CELL = 8   # heat, forward Euler: 2 FMA, 4 add, 2 multiply (numpy's order)
 FP64_LANES_PER_SM = 64  # B200: 148 SMs x 64 FP64 lanes x 1965 MHz = 18.6 T FP64 instructions/s
 
 
+def max_sm_mhz(clk):
+    """The GPU's maximum SM clock: sampled by nvidia-smi during the run, else
+    the measured-peaks record, else B200's 1965 MHz."""
+    mhz = (clk or {}).get("sm_max_mhz")
+    if not mhz:
+        try:
+            mhz = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["sm_max_mhz"])
+        except (OSError, KeyError, ValueError):
+            mhz = 1965.0
+    return float(mhz)
+
+
 def fp64_roof(cells, ms, clk):
     """The swept streams are bound by FP64 issue, not HBM: FP64 instructions
-    per second of the dominant kernel against the FP64 pipe's rate at the
-    sampled SM clock (an FMA counts as one instruction)."""
+    per second of a kernel against the FP64 pipe's rate (64 lanes per SM) at
+    the GPU's maximum SM clock (an FMA counts as one instruction), in
+    T instructions/s.  The rate at the sampled median clock is reported
+    beside it."""
     import torch
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
-    achieved = cells * FP64_OPS_PER_CELL / (ms / 1000) / 1e9
-    peak = sms * FP64_LANES_PER_SM * mhz * 1e6 / 1e9
-    return {"ops_per_cell": FP64_OPS_PER_CELL, "achieved_ginstr_s": achieved,
-            "peak_ginstr_s": peak, "frac": achieved / peak, "sm_mhz": mhz}
+    mhz = max_sm_mhz(clk)
+    achieved = cells * FP64_OPS_PER_CELL / (ms / 1000) / 1e12
+    peak = sms * FP64_LANES_PER_SM * mhz * 1e6 / 1e12
+    med = (clk or {}).get("sm_mhz")
+    out = {"ops_per_cell": FP64_OPS_PER_CELL, "achieved": achieved, "peak": peak,
+           "frac": achieved / peak, "sm_max_mhz": mhz}
+    if med:
+        out["frac_at_median_clock"] = achieved / (peak * med / mhz)
+        out["sm_median_mhz"] = med
+    return out
 
 
 def ncu_traffic(kind, n, bs, h):
     """DRAM bytes per launch of one kernel kind (h levels per half-cycle),
-    from a committed ncu summary."""
+    measured by ncu at this grid size and committed as a profile summary;
+    None where no capture of this size exists."""
     p = os.path.join(ROOT, "profiles", f"heat2d_swept_{kind}_traffic.txt")
     try:
         for line in open(p):
@@ -231,6 +258,39 @@ def workload_config(args):
             "l2": "inputs larger than L2 (field of n*n*8 bytes)"}
 
 
+def roofline(prof, cell_bytes, clk, traffic_key=None):
+    """Roofline of the dominant kernel of a run, from the per-launch CUDA-event
+    profile {kind: (ms, launches, cell updates)}.
+
+    The swept streams reuse every loaded value across the levels of a
+    half-cycle, so their binding resource is the FP64 pipe, not HBM: `bound`,
+    `achieved`, `peak` and `frac` are FP64 instructions per second against the
+    pipe's rate at the maximum SM clock.  `effective_bytes` keeps the
+    16-bytes-per-cell-update figure (a read and a write of each value) against
+    the measured HBM copy bandwidth, which exceeds 1 by the temporal reuse, and
+    `traffic` the DRAM bytes per launch that ncu measured at this size."""
+    kinds = {k: v for k, v in prof.items() if v[1] > 0}
+    dom = max(kinds, key=lambda k: kinds[k][0])
+    dms, dn, dcells = kinds[dom]
+    eff = dcells * cell_bytes / (dms / 1000) / 1e9
+    peak_bw, peak_src = measured_peak()
+    fp = fp64_roof(dcells, dms, clk)
+    traffic = ncu_traffic(dom, *traffic_key) if traffic_key else None
+    return {"bound": "fp64_pipe", "achieved": fp["achieved"], "peak": fp["peak"],
+            "unit": "T FP64 instructions/s", "frac": fp["frac"], "traffic": traffic,
+            "traffic_gbs": traffic / (dms / dn / 1000) / 1e9 if traffic else None,
+            "kernel": dom, "launches": dn, "avg_launch_ms": dms / dn,
+            "cell_updates_per_launch": dcells / dn, "fp64": fp,
+            "effective_bytes": {"achieved": eff, "peak": peak_bw, "unit": "GB/s",
+                                "frac": eff / peak_bw, "bytes_per_cell_update": cell_bytes,
+                                "peak_source": peak_src,
+                                "algorithmic_bytes_per_launch": dcells * cell_bytes / dn},
+            "effective_bytes_frac": eff / peak_bw,
+            "kernel_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()},
+            "per_kernel": {k: dict(fp64_roof(v[2], v[0], clk), avg_launch_ms=v[0] / v[1],
+                                   launches=v[1]) for k, v in kinds.items()}}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -302,6 +362,10 @@ def run_b200(args):
     ms_sw, launches, prof = timed("swept", args.steps)
     clk = clocks.stop()
     value = cells_per_step * world / (ms_sw / 1000) / 1e9
+    # the swept result of the timed solves, kept on the device for the
+    # bitwise comparison with the standard decomposition's
+    swept_out = torch.empty_like(d_ic)
+    eng.get_state(out=swept_out)
 
     std = None
     if args.standard_steps > 0:
@@ -313,6 +377,11 @@ def run_b200(args):
         pk = prof_st["standard"]
         if pk[1]:
             std["kernel_effective_gbs"] = pk[2] * cell_bytes / (pk[0] / 1000) / 1e9
+        std_out = torch.empty_like(d_ic)
+        eng.get_state(out=std_out)
+        torch.cuda.synchronize()
+        std["swept_equals_standard"] = bool(torch.equal(swept_out, std_out))
+        del std_out
 
     # end to end through the public API with pinned host buffers
     h_in = torch.from_numpy(ic).pin_memory()
@@ -336,20 +405,7 @@ def run_b200(args):
            "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8),
            "ms_per_step": ms_e2e, "steps": args.e2e_steps}
 
-    # roofline of the dominant kernel
-    kinds = {k: v for k, v in prof.items() if v[1] > 0}
-    dom = max(kinds, key=lambda k: kinds[k][0])
-    dms, dn, dcells = kinds[dom]
-    achieved = dcells * cell_bytes / (dms / 1000) / 1e9
-    peak, peak_src = measured_peak()
-    traffic = None if f32 else ncu_traffic(dom, n, bs, eng.tiling()["h"])
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "kernel": dom,
-            "launches": dn, "avg_launch_ms": dms / dn,
-            "algorithmic_bytes_per_launch": dcells * cell_bytes / dn,
-            "peak_source": peak_src,
-            "kernel_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()},
-            "fp64": fp64_roof(dcells, dms, clk)}
+    roof = roofline(prof, cell_bytes, clk, None if f32 else (n, bs, eng.tiling()["h"]))
 
     cfg = workload_config(args)
     if f32:
@@ -360,6 +416,7 @@ def run_b200(args):
             "dtype": "f32 storage, f64 arithmetic" if f32 else "f64",
             "data": "synthetic", "config": cfg, "standard": std,
             "swept_vs_standard": (value / std["value"]) if std else None,
+            "swept_equals_standard": std["swept_equals_standard"] if std else None,
             "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
             "tiling": dict(eng.tiling(), nseg_auto=not args.nseg)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not f32:
@@ -370,12 +427,42 @@ def run_b200(args):
             "sample": f"{args.ref_n}x{args.ref_n} heat, bs {bs}, {args.ref_cycles} swept "
                       f"half-cycles, {secs:.1f} s"}
         line["parity"] = parity_check(sample, bs, local)
+    eng.close()
+    del d_ic, swept_out
+    if rank == 0 and world == 1 and not args.no_secondary and not f32:
+        torch.cuda.empty_cache()
+        line["secondary"] = secondary_lines(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def secondary_lines(args):
+    """The other targets of the metric, on the same GPU after the headline:
+    Euler swept vs standard (4096^2, blocksize 16, 1000 steps), the adjoint's
+    cost against its forward pass (2048^2, 2000 steps, 32 finite-difference
+    directions) and the batched instances against one solver per instance
+    (256 heat instances for 1000 steps; the 64 Euler instances for
+    SECONDARY_EULER_BATCH_STEPS steps; one timed run of each side, to keep the
+    default run within a few minutes)."""
+    import copy
+
+    import torch
+    out = {}
+    # the batched comparison builds 320 solvers per timing: one warm-up and
+    # one timed run of each side
+    quick = copy.copy(args)
+    quick.steps, quick.warmup = 1, 1
+    for name, fn in (("euler", lambda: euler_line(args)),
+                     ("adjoint", lambda: adjoint_line(args)),
+                     ("batched", lambda: batched_line(quick, SECONDARY_EULER_BATCH_STEPS))):
+        t0 = time.perf_counter()
+        out[name] = fn()
+        out[name]["wall_s"] = time.perf_counter() - t0
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_b200_slabs(args):
@@ -451,16 +538,7 @@ def run_b200_slabs(args):
     e2e = {"value": cells_per_step * world / (ms_e2e / 1000) / 1e9, "unit": UNIT,
            "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8),
            "ms_per_step": ms_e2e, "steps": args.e2e_steps}
-    kinds = {k: v for k, v in prof.items() if v[1] > 0}
-    dom = max(kinds, key=lambda k: kinds[k][0])
-    dms, dn, dcells = kinds[dom]
-    achieved = dcells * CELL_BYTES / (dms / 1000) / 1e9
-    peak, peak_src = measured_peak()
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "kernel": dom, "launches": dn,
-            "avg_launch_ms": dms / dn, "algorithmic_bytes_per_launch": dcells * CELL_BYTES / dn,
-            "peak_source": peak_src,
-            "kernel_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()}}
+    roof = roofline(prof, CELL_BYTES, clk)
     cfg = workload_config(args)
     cfg.update({"workload": f"heat2d-fp64-periodic-{n * world}x{n}-{steps}steps-swept-slabs",
                 "global_rows": n * world, "rows_per_gpu": n, "halo_rows": bs // 2,
@@ -494,8 +572,13 @@ def euler_field(n, seed=0, modes=8, gamma=1.4):
 
 
 def run_euler(args):
+    print(json.dumps(euler_line(args)), flush=True)
+    return 0
+
+
+def euler_line(args):
     """Euler swept vs standard on one GPU (vortex-free periodic field of Fourier
-    modes, CFL 0.1, two RK stages per step); one JSON line."""
+    modes, CFL 0.1, two RK stages per step)."""
     import torch
 
     from pysweep_b200 import Engine, plugin_constants
@@ -543,9 +626,8 @@ def run_euler(args):
             "n": n, "time_steps": steps, "blocksize": bs, "chunk": args.euler_chunk or "default",
             "stages_per_step": 2,
             "dtype": "f64", "data": "synthetic", "steps": args.steps}
-    print(json.dumps(line), flush=True)
     eng.close()
-    return 0
+    return line
 
 
 def batched_instances(seed=1, n_heat=256, n_euler=64):
@@ -559,7 +641,13 @@ def batched_instances(seed=1, n_heat=256, n_euler=64):
 
 
 def run_batched(args):
-    """Batched persistent launches (one CUDA graph) vs one solver per instance."""
+    print(json.dumps(batched_line(args)), flush=True)
+    return 0
+
+
+def batched_line(args, euler_steps=None):
+    """Batched persistent launches (one CUDA graph) vs one solver per instance.
+    euler_steps: time steps of the Euler group (default: the heat group's)."""
     import torch
 
     from pysweep_b200 import Engine, plugin_constants
@@ -576,7 +664,8 @@ def run_batched(args):
             continue
         its = 1 if eqn == "heat" else 2
         bs = 32 if eqn == "heat" else 16
-        nl = args.batched_steps * its
+        tsteps = args.batched_steps if (eqn == "heat" or not euler_steps) else euler_steps
+        nl = tsteps * its
         fields, consts = [], []
         for n, par in inst:
             if eqn == "heat":
@@ -650,7 +739,7 @@ def run_batched(args):
         for e in engines:
             e.close()
         best = min(res.values())
-        groups.append({"equation": eqn, "instances": len(inst), "time_steps": args.batched_steps,
+        groups.append({"equation": eqn, "instances": len(inst), "time_steps": tsteps,
                        "blocksize": bs, "batched_s": t_batch, "per_instance_one_stream_s": res["one_stream"],
                        "per_instance_own_streams_s": res["own_streams"],
                        "speedup_vs_best_per_instance": best / t_batch,
@@ -661,11 +750,15 @@ def run_batched(args):
     out["value_vs_own_streams"] = (sum(g["per_instance_own_streams_s"] for g in groups) /
                                    sum(g["batched_s"] for g in groups))
     out["timing"] = "wall clock around the run with device synchronisation on both sides"
-    print(json.dumps(out), flush=True)
-    return 0
+    return out
 
 
 def run_adjoint(args):
+    print(json.dumps(adjoint_line(args)), flush=True)
+    return 0
+
+
+def adjoint_line(args):
     """Inverse heat problem: forward vs adjoint cost, gradients vs central differences."""
     import torch
 
@@ -734,13 +827,12 @@ def run_adjoint(args):
         worst = max(worst, abs(d(h) - an) / max(abs(an), 1e-300))
         worst_r = max(worst_r, abs((4 * d(hr / 2) - d(hr)) / 3 - an) / max(abs(an), 1e-300))
     t_f, t_b = statistics.median(fwd), statistics.median(bwd)
-    print(json.dumps({
+    return {
         "metric": "adjoint/forward cost", "value": t_b / t_f, "unit": "x", "higher_is_better": False,
         "forward_ms": t_f, "backward_ms": t_b, "n": n, "time_steps": steps, "checkpoint_every": every,
         "fd_directions": args.adj_dirs, "fd_h": h, "fd_max_rel_err": worst,
         "fd_richardson_h": hr, "fd_richardson_max_rel_err": worst_r, "dtype": "f64",
-        "data": "synthetic", "steps": args.steps, "warmup": args.warmup}), flush=True)
-    return 0
+        "data": "synthetic", "steps": args.steps, "warmup": args.warmup}
 
 
 def main():
@@ -759,6 +851,8 @@ def main():
     ap.add_argument("--ref-n", type=int, default=2048)
     ap.add_argument("--ref-cycles", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the Euler, adjoint and batched lines of the default run")
     ap.add_argument("--f32", action="store_true",
                     help="float32 fields (the reference's dtype: float32) on one GPU")
     ap.add_argument("--batched", action="store_true",

@@ -74,6 +74,39 @@ int ps_create(ps_solver **out, int device, int equation, int nv, int nx, int ny,
 int ps_create_typed(ps_solver **out, int device, int equation, int nv, int nx, int ny, int ops,
                     int its, int blocksize, int dtype);
 
+/*
+ * Create a solver whose step function is a user hook compiled at run time:
+ * `source` is the text of a plugin's .cu file that defines
+ *     __device__ void step(double *shared_state, int idx, int globalTimeStep)
+ * and its own __device__ __constant__ globals, exactly as the reference's
+ * plugins do (pysweep/equations/*.cu); `name` labels it in compiler messages.
+ * Replaces io.buildGPUSource (pysweep/core/io.py:146-155), which includes the
+ * file into pysweep.cu (pysweep/core/pysweep.cu:25) and builds it with PyCUDA.
+ * The hook sees the framework constants of pysweep/core/pysweep.cu:12-20 (VARS,
+ * TIMES, MPSS, MOSS, NV, OPS, ITS, SX, SY): variable v of its cell is
+ * shared_state[idx + v*VARS], the neighbours are idx +- SY (x, rows) and
+ * idx +- 1 (y, columns) up to OPS away, the previous level is idx - TIMES
+ * (its own cell only) and it writes the next level at idx + TIMES.  It is
+ * compiled with NVRTC for sm_100a with --fmad=false (every operation rounded
+ * separately); the swept and standard decompositions run the same compiled
+ * hook, so their results are bitwise equal.  Its constants are set by name
+ * with ps_set_global (the value is converted to the declared type).  On a
+ * compiler error the call returns PS_ERR_COMPILE and ps_last_error(NULL)
+ * holds the compiler's log.  nv in 1..8, ops in 1..4, its in 1..2; fields are
+ * float64.  The levels per half-cycle default to MPSS, or fewer where the
+ * tiles of one level per slot would not fit in shared memory.
+ */
+int ps_create_hook(ps_solver **out, int device, const char *source, const char *name, int nv,
+                   int nx, int ny, int ops, int its, int blocksize);
+
+/*
+ * Compile a step hook without a device (the check io.buildGPUSource's
+ * SourceModule performs at Solver start, pysweep/core/io.py:146-155): PS_OK, or
+ * PS_ERR_COMPILE with the compiler's log in `log` (loglen bytes at most).
+ */
+int ps_hook_check(const char *source, const char *name, int nv, int ops, int its, char *log,
+                  size_t loglen);
+
 /* Release everything the solver owns.  Replaces process.cleanupProcesses'
  * context pop (pysweep/core/process.py:28-33). */
 int ps_destroy(ps_solver *s);
@@ -195,13 +228,15 @@ const char *ps_last_error(const ps_solver *s);
  * that cannot call cudaMalloc at the time they solve -- a process whose memory
  * pool already owns the device memory, a real-time loop that must not touch
  * the allocator.  The caller
- * passes the input and output fields (device pointers, nx*ny doubles, distinct);
+ * passes the input and output fields (device pointers, nx*ny doubles, not
+ * overlapping each other or the scratch array; overlaps are rejected);
  * every temporary lives in one static device array of 128 MiB that each GPU
  * holds from library load to process exit.  Sizes whose scratch (one field plus
  * the prism faces, about 22*nx*ny bytes at blocksize 32) exceeds it are
  * rejected with PS_ERR_INVALID and a message in err.  The first call on a
  * device resolves the array's device address, so make it before any stream
- * capture.  Calls share the array: two calls that overlap on the GPU (other
+ * capture; that address is kept for the life of the process, so a
+ * cudaDeviceReset after the first call is not supported.  Calls share the array: two calls that overlap on the GPU (other
  * streams, other host threads) race and corrupt each other.  No part of the
  * array needs to start at zero (every half-cycle writes what it reads).
  * Computes nsteps steps of courant = alpha*dt/dx/dx on `stream` (NULL = the
@@ -218,7 +253,11 @@ int ps_heat_swept_noalloc(const double *d_in, double *d_out, int nx, int ny, int
  * phase of a half-cycle is one launch for all instances (a flat table of
  * (instance, band segment) units); with use_graph != 0 the launches of a whole
  * run are captured once into a CUDA graph and replayed.  Constants are per
- * instance (index) or for all (index = -1).  Register streams (heat, forward
+ * instance (index) or for all (index = -1).  Each instance counts the levels
+ * run since its state was set: the first level after ps_batch_set_state sees
+ * globalTimeStep = 1 (pysweep/core/solver.py:162) and consecutive
+ * ps_batch_run calls continue the count, so runs of any length (odd ones with
+ * two stages included) add up to one run of their total.  Register streams (heat, forward
  * Euler, blocksize 16/32) need nx, ny multiples of 32; the other equations use
  * the shared-memory streams with one segment per band.
  */

@@ -7,7 +7,7 @@ the Python side of that ABI and the drop-in ``Solver`` front-end.
 """
 from ._lib import PySweepError  # noqa: F401
 from .batch import Batch  # noqa: F401
-from .engine import Engine, plugin_constants  # noqa: F401
+from .engine import Engine, check_hook, plugin_constants  # noqa: F401
 
 __version__ = "0.1.0"
 

@@ -38,6 +38,11 @@ _SIGS = {
     "ps_create_typed": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "ps_create_hook": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                      ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "ps_hook_check": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
     "ps_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "ps_set_global": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p,
                                      ctypes.c_size_t]),

@@ -38,7 +38,7 @@ def build(force=False, verbose=False):
     if not force and not _stale():
         return LIB
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    cmd = [nvcc()] + ARCH + FLAGS + ["-o", LIB + ".tmp"] + srcs + ["-lcuda"]
+    cmd = [nvcc()] + ARCH + FLAGS + ["-o", LIB + ".tmp"] + srcs + ["-ldl"]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

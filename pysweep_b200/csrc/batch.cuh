@@ -38,7 +38,8 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3)
     const int2 u = units[g];
     SweptArgs a;
     batch_args<GAP>(desc, u.x, parity, H, L0, a);
-    heat_fast_body<BX, GAP>(a, u.y, sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
+    heat_fast_body<BX, GAP>(a, seg_geom(a, u.y), u.y,
+                            sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
 // The generic batched kernels hold the descriptor fields in registers (the

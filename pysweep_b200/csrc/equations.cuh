@@ -20,7 +20,9 @@
 // The library is compiled with --fmad=false; fma() appears only where it is
 // exactly equal to the separately rounded expression (a - 2*c: 2*c is exact).
 #pragma once
+#ifndef __CUDACC_RTC__  // run-time compilation (user step hooks) has no host headers
 #include <cuda_runtime.h>
+#endif
 
 namespace psb {
 

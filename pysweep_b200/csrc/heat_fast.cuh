@@ -283,22 +283,24 @@ __device__ __forceinline__ void gap_entry(const double (&a1)[BX], const double* 
     }
 }
 
-// One (band, segment) unit of one warp; `carry` is the warp's own shared
-// memory (heat_fast_warp_doubles: two packed carry buffers, then the ring).
+// One column segment of one band, run by one warp; `unit` indexes the
+// segment's y-faces; `carry` is the warp's own shared memory
+// (heat_fast_warp_doubles: two packed carry buffers, then the ring).
 // T: storage type of the fields and faces (double or float).
 template <int BX, bool GAP, class T = double>
-__device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int unit, double* carry)
+__device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom sg,
+                                               const int unit, double* carry)
 {
     using P = typename Pair2<T>::type;
     constexpr int hx = BX / 2;
     const int lane = threadIdx.x & 31;
     const int H = a.H, Hm = a.Hmax, nx = a.nx, ny = a.ny;
-    const int band = unit / a.nseg, seg = unit % a.nseg;
+    const int band = sg.band;
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
-    const int s0 = seg_start(a, seg);
+    const int s0 = sg.s0;
     // segments are whole multiples of 32 columns: 64-column chunks, the last
     // one possibly 32 wide (lanes 16..31 then hold columns past the segment)
-    const int wseg = seg_start(a, seg + 1) - s0;
+    const int wseg = sg.s1 - s0;
     const int nchunks = (wseg + kFastChunk - 1) / kFastChunk;
     const int lastw = wseg - (nchunks - 1) * kFastChunk;
     const double cr = a.p.d[0];
@@ -518,14 +520,27 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const int uni
     }
 }
 
+// Warps of a stream launch: one per segment, or, with a segment table, one
+// per equal share of the grid's columns (its segments in turn).
+__host__ __device__ inline int stream_units(const SweptArgs& a)
+{
+    return a.segs ? a.nunits : a.nb * a.nseg;
+}
+
 template <int BX, bool GAP, class T = double>
 __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs a)
 {
     extern __shared__ double sm[];
     const int warp = threadIdx.x >> 5;
     const int unit = blockIdx.x * kFastWarps + warp;
-    if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
-    heat_fast_body<BX, GAP, T>(a, unit, sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
+    if (unit >= stream_units(a)) return;  // whole warp leaves together
+    double* carry = sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax);
+    if (!a.segs) {
+        heat_fast_body<BX, GAP, T>(a, seg_geom(a, unit), unit, carry);
+        return;
+    }
+    for (int i = a.ufirst[unit]; i < a.ufirst[unit + 1]; ++i)
+        heat_fast_body<BX, GAP, T>(a, seg_geom(a, i), i, carry);
 }
 
 }  // namespace psb

@@ -39,6 +39,13 @@ void put_err(char* err, size_t errlen, const char* msg)
 
 size_t round_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// Whether the byte ranges [a, a+na) and [b, b+nb) share a byte.
+bool overlap(const void* a, size_t na, const void* b, size_t nb)
+{
+    const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+    return x < y + nb && y < x + na;
+}
+
 }  // namespace
 
 using namespace psb;
@@ -48,8 +55,8 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
                                      double dx, void* stream, char* err, size_t errlen)
 {
     char msg[256];
-    if (!d_in || !d_out || d_in == d_out) {
-        put_err(err, errlen, "d_in and d_out must be distinct device pointers");
+    if (!d_in || !d_out) {
+        put_err(err, errlen, "d_in and d_out must be device pointers");
         return PS_ERR_INVALID;
     }
     if ((blocksize != 16 && blocksize != 32) || nx <= 0 || ny <= 0 || nx % blocksize ||
@@ -63,15 +70,6 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
     }
     cudaStream_t st = (cudaStream_t)stream;
     const size_t fe = (size_t)nx * ny;
-    if (nsteps == 0) {
-        cudaError_t e = cudaMemcpyAsync(d_out, d_in, fe * sizeof(double),
-                                        cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) {
-            put_err(err, errlen, cudaGetErrorString(e));
-            return PS_ERR_CUDA;
-        }
-        return PS_OK;
-    }
     // tiling: the defaults of a ps_solver (MPSS levels per half-cycle, one
     // wave of warps); results do not depend on it
     int dev = 0;
@@ -92,6 +90,19 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
         put_err(err, errlen, msg);
         return PS_ERR_INVALID;
     }
+    if (overlap(d_in, fe * sizeof(double), d_out, fe * sizeof(double))) {
+        put_err(err, errlen, "d_in and d_out overlap: the solve reads d_in while it writes d_out");
+        return PS_ERR_INVALID;
+    }
+    if (nsteps == 0) {
+        cudaError_t e = cudaMemcpyAsync(d_out, d_in, fe * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) {
+            put_err(err, errlen, cudaGetErrorString(e));
+            return PS_ERR_CUDA;
+        }
+        return PS_OK;
+    }
     if (dev < 0 || dev >= kMaxDevices) {
         put_err(err, errlen, "device ordinal out of range");
         return PS_ERR_INVALID;
@@ -109,18 +120,27 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
                 put_err(err, errlen, msg);
                 return PS_ERR_CUDA;
             }
-            auto k0 = heat_stream_fast<16, false>, k1 = heat_stream_fast<16, true>;
-            auto k2 = heat_stream_fast<32, false>, k3 = heat_stream_fast<32, true>;
-            auto k4 = seam_kernel<Heat, 1, false, 128>, k5 = seam_kernel<Heat, 1, true, 128>;
-            cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-            cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-            cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-            cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-            cudaFuncSetAttribute(k4, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-            cudaFuncSetAttribute(k5, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+            const void* kernels[] = {
+                (const void*)heat_stream_fast<16, false>, (const void*)heat_stream_fast<16, true>,
+                (const void*)heat_stream_fast<32, false>, (const void*)heat_stream_fast<32, true>,
+                (const void*)seam_kernel<Heat, 1, false, 128>,
+                (const void*)seam_kernel<Heat, 1, true, 128>};
+            for (const void* k : kernels) {
+                e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+                if (e != cudaSuccess) {
+                    snprintf(msg, sizeof msg, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+                    put_err(err, errlen, msg);
+                    return PS_ERR_CUDA;  // the device stays unset: the next call retries
+                }
+            }
             g_scratch_ptr[dev] = p;
         }
         base = g_scratch_ptr[dev];
+    }
+    if (overlap(d_in, fe * sizeof(double), base, need) ||
+        overlap(d_out, fe * sizeof(double), base, need)) {
+        put_err(err, errlen, "d_in or d_out lies inside the library's scratch array");
+        return PS_ERR_INVALID;
     }
     double* A = (double*)base;
     SweptArgs a;

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -17,6 +18,7 @@
 #include "standard_fast.cuh"
 #include "euler_faces.cuh"
 #include "batch.cuh"
+#include "hook.cuh"
 
 namespace psb {
 
@@ -92,6 +94,17 @@ struct ps_solver {
     int64_t prof_n[8] = {0};
     // algorithmic cell updates per kernel kind, accumulated with prof_ms
     double prof_cells[8] = {0};
+    // user step hook compiled at run time (ps_create_hook); nullptr for the
+    // built-in equations
+    HookModule* hook = nullptr;
+    // register streams in automatic tiling: the balanced segment table
+    // (build_seg_table); seg_table false = nseg equal segments per band
+    bool seg_table = false;
+    int4* d_segs = nullptr;
+    int* d_ufirst = nullptr;
+    int seg_total = 0, seg_units = 0;
+    std::string hook_src;    // the hook's source (declared types of its constants)
+    std::string launch_err;  // a driver-API launch failure, reported by check_launch
 };
 
 namespace {
@@ -120,12 +133,15 @@ void allow_big_smem(K kernel)
 int fail(ps_solver* s, int code, const char* fmt, ...)
 {
     if (s) {
-        char buf[512];
-        va_list ap;
+        va_list ap, ap2;
         va_start(ap, fmt);
-        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_copy(ap2, ap);
+        const int n = vsnprintf(nullptr, 0, fmt, ap);
         va_end(ap);
-        s->err = buf;
+        std::string buf(n > 0 ? (size_t)n : 0, '\0');
+        if (n > 0) vsnprintf(&buf[0], (size_t)n + 1, fmt, ap2);
+        va_end(ap2);
+        s->err = buf;  // any length: hook compiler logs included
     }
     return code;
 }
@@ -192,8 +208,11 @@ EqParams make_params_g(int eq, const std::map<std::string, double>& globals)
 
 EqParams make_params(const ps_solver* s) { return make_params_g(s->eq, s->globals); }
 
+// Equation id of solvers running a user step hook (internal: ps_create_hook)
+constexpr int PS_EQ_HOOK = 5;
+
 // ------------------------------------------------------------ dispatch ----
-using SweptLaunch = void (*)(const SweptArgs&, int grid, size_t smem, cudaStream_t);
+using SweptLaunch = std::function<void(const SweptArgs&, int grid, size_t smem, cudaStream_t)>;
 using StdLaunch = void (*)(const double*, const double*, double*, double*, int, int, int, int,
                            const EqParams&, cudaStream_t);
 
@@ -235,7 +254,7 @@ void launch_fast(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
 {
     auto k = heat_stream_fast<BX, GAP, T>;
     allow_big_smem(k);
-    const int units = a.nb * a.nseg;
+    const int units = stream_units(a);
     k<<<(units + kFastWarps - 1) / kFastWarps, 32 * kFastWarps, smem, st>>>(a);
 }
 
@@ -291,6 +310,11 @@ StdLaunch pick_standard(int eq, int ops)
 
 int check_launch(ps_solver* s)
 {
+    if (!s->launch_err.empty()) {
+        const std::string m = s->launch_err;
+        s->launch_err.clear();
+        return fail(s, PS_ERR_CUDA, "kernel launch: %s", m.c_str());
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(s, PS_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
     s->launches++;
@@ -346,6 +370,61 @@ int drain_profile(ps_solver* s)
     return PS_OK;
 }
 
+// Balanced segments for the register streams: the grid's 32-column units,
+// band after band, cut into `slots` equal shares, one per stream warp, each
+// share cut again at band boundaries into segments.  With equal segments per
+// band the warps number nb * nseg, which rarely fills the GPU's warp slots
+// (8192^2 at bs 32: 256 bands x 6 segments = 1536 warps for 1776 slots, and 7
+// segments would need a second wave); equal shares fill every slot with the
+// same work, for some 30% more segments (seams).  Segments are numbered band
+// after band, so each segment's left neighbour is the one before it, or the
+// band's last one.
+int build_seg_table(ps_solver* s, int slots)
+{
+    const int nb = s->nx / s->bs, per = s->ny / 32;
+    const long long T = (long long)nb * per;
+    // shares of at least two units (64 columns) where the grid is small
+    const int U = (int)std::max<long long>(1, std::min<long long>(slots, T / 2));
+    if (s->seg_table && s->seg_units == U) return PS_OK;
+    std::vector<int4> segs;
+    std::vector<int> ufirst(U + 1);
+    std::vector<int> band_first(nb, -1);
+    for (int u = 0; u < U; ++u) {
+        ufirst[u] = (int)segs.size();
+        long long p = T * u / U;
+        const long long p1 = T * (u + 1) / U;
+        while (p < p1) {
+            const int band = (int)(p / per);
+            const long long e = std::min<long long>(p1, (long long)(band + 1) * per);
+            if (band_first[band] < 0) band_first[band] = (int)segs.size();
+            segs.push_back(make_int4(band, (int)(p - (long long)band * per) * 32,
+                                     (int)(e - (long long)band * per) * 32, 0));
+            p = e;
+        }
+    }
+    ufirst[U] = (int)segs.size();
+    for (size_t i = 0; i < segs.size(); ++i) {
+        const int b = segs[i].x;
+        const size_t last = (b + 1 < nb ? (size_t)band_first[b + 1] : segs.size()) - 1;
+        segs[i].w = segs[i].y == 0 ? (int)last : (int)i - 1;
+    }
+    if (s->d_segs) cudaFree(s->d_segs);
+    if (s->d_ufirst) cudaFree(s->d_ufirst);
+    s->d_segs = nullptr;
+    s->d_ufirst = nullptr;
+    s->seg_table = false;
+    PS_CUDA(s, cudaMalloc(&s->d_segs, segs.size() * sizeof(int4)));
+    PS_CUDA(s, cudaMalloc(&s->d_ufirst, ufirst.size() * sizeof(int)));
+    PS_CUDA(s, cudaMemcpy(s->d_segs, segs.data(), segs.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    PS_CUDA(s, cudaMemcpy(s->d_ufirst, ufirst.data(), ufirst.size() * sizeof(int),
+                          cudaMemcpyHostToDevice));
+    s->seg_table = true;
+    s->seg_units = U;
+    s->seg_total = (int)segs.size();
+    s->nseg = (s->seg_total + nb - 1) / nb;  // reported: segments per band, rounded up
+    return PS_OK;
+}
+
 int ensure_swept_buffers(ps_solver* s)
 {
     const int O2 = 2 * s->ops;
@@ -353,8 +432,9 @@ int ensure_swept_buffers(ps_solver* s)
     const int HF = std::max(s->H - 1, 0);
     const size_t xn = (size_t)nb * HF * 2 * s->nv * O2 * s->ny;
     // two y-face buffers: prism -> y-bridge, gap -> octahedron (the y-bridge
-    // and the gap stream run at the same time)
-    const size_t yn = 2 * (size_t)nb * s->nseg * 2 * HF * s->nv * s->bs * O2;
+    // and the gap stream run at the same time), one pair of sides per segment
+    const size_t nsegs = s->seg_table ? (size_t)s->seg_total : (size_t)nb * s->nseg;
+    const size_t yn = 2 * nsegs * 2 * HF * s->nv * s->bs * O2;
     if (xn > s->xface_n) {
         if (s->xface) cudaFree(s->xface);
         s->xface = nullptr;
@@ -383,10 +463,14 @@ int default_levels(int eq, int its, int bs, int mpss)
     return mpss;
 }
 
+// tile slots of the stream and seam kernels: a ring of its+1 for the built-in
+// equations, levels -1 .. Hmax for a step hook (slot_count in swept.cuh)
+int tile_slots(const ps_solver* s) { return s->hook ? s->H + 2 : s->its + 1; }
+
 size_t stream_tile_smem(const ps_solver* s)
 {
     const int O2 = 2 * s->ops, RS = s->chunk + O2;
-    return s->esize * ((size_t)(s->its + 1) * s->nv * s->bs * RS +
+    return s->esize * ((size_t)tile_slots(s) * s->nv * s->bs * RS +
                        (size_t)(s->H + 1) * s->nv * s->bs * O2);
 }
 
@@ -407,12 +491,59 @@ size_t stream_smem(const ps_solver* s)
            (euler_faces_fit(s) ? sizeof(double) * euler_level_scratch(s->bs, s->chunk) : 0);
 }
 
+bool solver_seam_direct(const ps_solver* s)
+{
+    return seam_direct(s->bs, s->ops, s->nv, s->its, s->H, s->esize, tile_slots(s));
+}
+
 size_t seam_smem(const ps_solver* s)
 {
-    if (seam_direct(s->bs, s->ops, s->nv, s->its, s->H, s->esize))
-        return s->esize * (size_t)(s->its + 1) * s->nv * s->bs * (2 * s->ops * (s->H + 1));
-    return s->esize * std::max(seam_smem_elems(false, s->bs, s->ops, s->nv, s->its, s->H),
-                               seam_smem_elems(true, s->bs, s->ops, s->nv, s->its, s->H));
+    const int ns = tile_slots(s);
+    if (solver_seam_direct(s))
+        return s->esize * (size_t)ns * s->nv * s->bs * (2 * s->ops * (s->H + 1));
+    return s->esize * std::max(seam_smem_elems(false, s->bs, s->ops, s->nv, s->its, s->H, ns),
+                               seam_smem_elems(true, s->bs, s->ops, s->nv, s->its, s->H, ns));
+}
+
+// ------------------------------------------------------------ step hooks ----
+// Driver-API launch of a hook kernel; a failure is kept for check_launch.
+void hook_launch(ps_solver* s, CUfunction f, int gx, int gy, int nt, size_t smem,
+                 cudaStream_t st, void** args)
+{
+    CUresult r = drv().launchKernel(f, gx, gy, 1, nt, 1, 1, (unsigned)smem, (CUstream)st, args,
+                                    nullptr);
+    if (r != CUDA_SUCCESS) s->launch_err = cu_error(r);
+}
+
+SweptSet hook_set(ps_solver* s)
+{
+    const int w = s->chunk == 64 ? 1 : 0;
+    HookModule* h = s->hook;
+    auto mk = [s](CUfunction f, int nt) {
+        return [s, f, nt](const SweptArgs& a, int grid, size_t smem, cudaStream_t st) {
+            SweptArgs copy = a;
+            void* args[] = {&copy};
+            hook_launch(s, f, grid, 1, nt, smem, st, args);
+        };
+    };
+    return SweptSet{mk(h->prism[w], 256), mk(h->ybridge, 128), mk(h->gap[w], 256),
+                    mk(h->octahedron, 128)};
+}
+
+// The framework constants of one kernel kind's tile (pysweep/core/pysweep.cu:
+// 12-20, set by io.copyConstants, io.py:169-184): a tile of `rows` x `cols`
+// cells per variable, levels `times` elements apart.
+int hook_frame(ps_solver* s, int ns, int rows, int cols, int times)
+{
+    HookModule* h = s->hook;
+    const int vals[FW_COUNT] = {rows * cols, times, s->mpss, 2 * s->mpss, s->nv,
+                                s->ops,      s->its, rows,   cols};
+    for (int f = 0; f < FW_COUNT; ++f) {
+        CUresult r = hook_set_fw(h, ns, f, vals[f], (CUstream)s->stream);
+        if (r != CUDA_SUCCESS)
+            return fail(s, PS_ERR_CUDA, "hook constant %s: %s", kHookFw[f], cu_error(r).c_str());
+    }
+    return PS_OK;
 }
 
 int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t frame_cap,
@@ -420,9 +551,12 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
 {
     SweptSet K;
     const int keq = (s->eq == PS_EQ_EULER && !euler_faces_fit(s)) ? PS_EQ_EULER_CELL : s->eq;
-    if (!pick_swept(keq, s->ops, s->its, s->chunk, &K))
+    if (s->hook) {
+        K = hook_set(s);
+    } else if (!pick_swept(keq, s->ops, s->its, s->chunk, &K)) {
         return fail(s, PS_ERR_UNSUPPORTED, "no swept kernels for equation %d ops %d its %d chunk %d",
                     s->eq, s->ops, s->its, s->chunk);
+    }
     const int O2 = 2 * s->ops;
     // register-resident streams for heat with forward Euler (the generic
     // seam kernels are shared)
@@ -438,7 +572,7 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         K.O = launch_seam<HeatF32, 1, true, float>;
         K.P = s->bs == 16 ? launch_fast<16, false, float> : launch_fast<32, false, float>;
         K.G = s->bs == 16 ? launch_fast<16, true, float> : launch_fast<32, true, float>;
-    } else if (s->eq == PS_EQ_HEAT && s->its == 1 && fwd_euler && s->threads != 256 &&
+    } else if (!s->hook && s->eq == PS_EQ_HEAT && s->its == 1 && fwd_euler && s->threads != 256 &&
                (s->bs == 16 || s->bs == 32) && s->ny % 32 == 0) {
         K.fast = true;
         if (s->bs == 16) {
@@ -462,15 +596,14 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     if (!K.fast && std::min(s->chunk, s->ny / s->nseg) < O2 * (s->H + 1))
         return fail(s, PS_ERR_INVALID, "segment width %d narrower than 2*ops*(h+1) = %d",
                     s->ny / s->nseg, O2 * (s->H + 1));
+    if (!s->nseg_auto || !K.fast) s->seg_table = false;
     if (s->nseg_auto) {
         if (K.fast) {
-            // one warp per (band, segment); 3 CTAs of 4 warps per SM fit
+            // one warp per equal share of the columns: 3 CTAs of 4 warps per SM fit
             int sms = 148;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-            const int slots = sms * 3 * kFastWarps;
-            const int nb = s->nx / s->bs;
-            s->nseg = std::max(1, std::min(s->ny / kFastChunk, slots / nb));
-            s->nseg = std::max(1, std::min(s->nseg, s->ny / 32));
+            int rc2 = build_seg_table(s, sms * 3 * kFastWarps);
+            if (rc2) return rc2;
         } else {
             // one CTA per (band, segment): the most segments that divide ny
             // and keep four chunks (and 2*ops*(h+1) columns) each.  Shorter
@@ -519,9 +652,25 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     a.gts_base = gts0 - 1;
     a.xface = s->xface;
     a.yface = s->yface;
+    if (s->seg_table) {
+        a.segs = s->d_segs;
+        a.ufirst = s->d_ufirst;
+        a.nunits = s->seg_units;
+        a.nsegs = s->seg_total;
+    }
     a.p = make_params(s);
-    a.seam_direct = seam_direct(s->bs, s->ops, s->nv, s->its, s->H, s->esize) ? 1 : 0;
-    const int units = a.nb * a.nseg;
+    a.seam_direct = solver_seam_direct(s) ? 1 : 0;
+    // seam CTAs: one per segment
+    const int units = s->seg_table ? s->seg_total : a.nb * a.nseg;
+    if (s->hook) {
+        // the hook's tiles: stream slots of bs rows x (chunk + 2 OPS) columns
+        // whose levels sit one slot + OPS apart (the chunk's parallelogram),
+        // seam slots of bs rows x 2 OPS (Hmax + 1) columns, one slot apart
+        const int rs = s->chunk + O2, tw = 2 * s->ops * (s->H + 1);
+        if ((rc = hook_frame(s, HOOK_STREAM, s->bs, rs, s->nv * s->bs * rs + s->ops)) ||
+            (rc = hook_frame(s, HOOK_SEAM, s->bs, tw, s->nv * s->bs * tw)))
+            return rc;
+    }
     const size_t fe = field_elems(s);
     int off = 0;
     int64_t done = 0;
@@ -543,7 +692,7 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         double cP = 0, cY = 0, cG = 0, cO = 0;
         for (int m = 1; m <= H; ++m) {
             const double rp = s->bs - 2.0 * s->ops * m, rg = 2.0 * s->ops * m;
-            const double cm = 2.0 * s->ops * m * s->nseg;  // seam columns of a band
+            const double cm = 2.0 * s->ops * m * units / a.nb;  // seam columns of a band
             const double cs = (double)s->ny - cm;           // stream columns of a band
             cP += rp * cs;
             cY += rp * cm;
@@ -576,8 +725,8 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
 int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t frame_cap,
                  int frame_every)
 {
-    StdLaunch K = pick_standard(s->eq, s->ops);
-    if (!K) return fail(s, PS_ERR_UNSUPPORTED, "no standard kernel for equation %d", s->eq);
+    StdLaunch K = s->hook ? nullptr : pick_standard(s->eq, s->ops);
+    if (!K && !s->hook) return fail(s, PS_ERR_UNSUPPORTED, "no standard kernel for equation %d", s->eq);
     const size_t fe = field_elems(s);
     for (int i = 0; i < 3; ++i)
         if (!s->ring[i]) PS_CUDA(s, cudaMalloc(&s->ring[i], nbytes(s, fe)));
@@ -601,6 +750,12 @@ int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_
         return fail(s, PS_ERR_UNSUPPORTED,
                     "float32 fields: heat with forward Euler and ny a multiple of 64 only");
     int rc;
+    if (s->hook) {
+        // the hook's standard tile: kHookStdTR x kHookStdTC cells and an
+        // OPS-cell halo per variable, previous / current / next level one slot apart
+        const int tr = kHookStdTR + 2 * s->ops, tc = kHookStdTC + 2 * s->ops;
+        if ((rc = hook_frame(s, HOOK_STD, tr, tc, s->nv * tr * tc))) return rc;
+    }
     for (int64_t L = 1; L <= nlevels; ++L) {
         double* fr = nullptr;
         if (frames && L % its == 0 && (L / its) % every == 0) {
@@ -609,7 +764,17 @@ int run_standard(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_
         }
         const int gts = gts0 + (int)(L - 1);
         if ((rc = timed_launch(s, 4, (double)s->nx * s->ny, [&] {
-                 if (fast) {
+                 if (s->hook) {
+                     const double* cur = s->ring[c];
+                     const double* prv = s->ring[p];
+                     double* nxt = s->ring[n];
+                     int nx = s->nx, ny = s->ny, g = gts;
+                     void* args[] = {&cur, &prv, &nxt, &fr, &nx, &ny, &g};
+                     const size_t tr = kHookStdTR + 2 * s->ops, tc = kHookStdTC + 2 * s->ops;
+                     hook_launch(s, s->hook->standard, (s->ny + kHookStdTC - 1) / kHookStdTC,
+                                 (s->nx + kHookStdTR - 1) / kHookStdTR, kHookStdNT,
+                                 3 * sizeof(double) * s->nv * tr * tc, s->stream, args);
+                 } else if (fast) {
                      const dim3 grid((s->ny / 64 + 7) / 8, (s->nx + kStdRows - 1) / kStdRows);
                      if (f32)
                          heat_standard_fast<false, float><<<grid, 256, 0, s->stream>>>(
@@ -687,6 +852,72 @@ double decode_value(const void* value, size_t nbytes)
     }
 }
 
+int solver_open(ps_solver* s);
+
+// Kind of a hook constant, from its declaration in the hook's source:
+// 'f' floating point, 'b' bool, 'i' any other (integer) type.
+char hook_const_kind(const std::string& src, const std::string& name)
+{
+    size_t pos = 0;
+    while ((pos = src.find("__constant__", pos)) != std::string::npos) {
+        const size_t end = src.find(';', pos);
+        if (end == std::string::npos) break;
+        const std::string decl = src.substr(pos, end - pos);
+        pos = end;
+        // the name as a whole word of the declaration
+        size_t k = 0;
+        bool found = false;
+        while ((k = decl.find(name, k)) != std::string::npos) {
+            const bool l = k == 0 || !(isalnum((unsigned char)decl[k - 1]) || decl[k - 1] == '_');
+            const size_t e = k + name.size();
+            const bool r = e >= decl.size() || !(isalnum((unsigned char)decl[e]) || decl[e] == '_');
+            if (l && r) {
+                found = true;
+                break;
+            }
+            k = e;
+        }
+        if (!found) continue;
+        if (decl.find("double") != std::string::npos || decl.find("float") != std::string::npos)
+            return 'f';
+        if (decl.find("bool") != std::string::npos) return 'b';
+        return 'i';
+    }
+    return 'f';
+}
+
+// The value in the representation of a hook constant of `size` bytes and
+// `kind` (the caller's bytes as they are when the sizes agree, else converted
+// through double).
+bool hook_encode(const void* value, size_t nbytes, size_t size, char kind, unsigned char* buf)
+{
+    if (nbytes == size) {
+        memcpy(buf, value, size);
+        return true;
+    }
+    const double d = decode_value(value, nbytes);
+    if (kind == 'f' && size == 8) {
+        memcpy(buf, &d, 8);
+    } else if (kind == 'f' && size == 4) {
+        const float f = (float)d;
+        memcpy(buf, &f, 4);
+    } else if (size == 8) {
+        const int64_t i = (int64_t)d;
+        memcpy(buf, &i, 8);
+    } else if (size == 4) {
+        const int32_t i = (int32_t)d;
+        memcpy(buf, &i, 4);
+    } else if (size == 2) {
+        const int16_t i = (int16_t)d;
+        memcpy(buf, &i, 2);
+    } else if (size == 1) {
+        buf[0] = kind == 'b' ? (d != 0.0) : (unsigned char)(int)d;
+    } else {
+        return false;
+    }
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -752,7 +983,25 @@ int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, i
         s->chunk = 64;
         if (stream_smem(s) > 227 * 1024) s->chunk = 32;
     }
+    if (rc == PS_OK) rc = solver_open(s);
+    if (rc != PS_OK) {
+        g_create_error = s->err;  // readable through ps_last_error(NULL)
+        ps_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return PS_OK;
+}
 
+}  // extern "C"
+
+namespace {
+
+// The device half of solver creation: device, stream, base buffers.
+int solver_open(ps_solver* s)
+{
+    const int device = s->device, nv = s->nv, nx = s->nx, ny = s->ny, its = s->its;
+    int rc = PS_OK;
     s->nseg = 1;
     if (rc == PS_OK) {
         cudaError_t e = cudaSetDevice(device);
@@ -770,8 +1019,84 @@ int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, i
             if (e != cudaSuccess) rc = fail(s, PS_ERR_NOMEM, "cudaMalloc base: %s", cudaGetErrorString(e));
         }
     }
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ps_hook_check(const char* source, const char* name, int nv, int ops, int its, char* log,
+                  size_t loglen)
+{
+    if (log && loglen) log[0] = '\0';
+    if (!source || nv < 1 || nv > 8 || ops < 1 || ops > 4 || its < 1 || its > 2)
+        return PS_ERR_INVALID;
+    std::vector<char> cubin;
+    std::string lg;
+    const int rc = hook_compile(hook_program(source, name ? name : "hook.cu", nv, ops, its), &cubin, &lg);
+    if (log && loglen) {
+        strncpy(log, lg.c_str(), loglen - 1);
+        log[loglen - 1] = '\0';
+    }
+    return rc;
+}
+
+int ps_create_hook(ps_solver** out, int device, const char* source, const char* name, int nv,
+                   int nx, int ny, int ops, int its, int blocksize)
+{
+    if (!out) return PS_ERR_INVALID;
+    *out = nullptr;
+    ps_solver* s = new ps_solver();
+    s->device = device;
+    s->eq = PS_EQ_HOOK;
+    s->nv = nv;
+    s->nx = nx;
+    s->ny = ny;
+    s->ops = ops;
+    s->its = its;
+    s->bs = blocksize;
+    int rc = PS_OK;
+    if (!source) rc = fail(s, PS_ERR_INVALID, "no hook source");
+    else if (nv < 1 || nv > 8 || ops < 1 || ops > 4 || its < 1 || its > 2)
+        rc = fail(s, PS_ERR_UNSUPPORTED, "step hooks: nv in 1..8, ops in 1..4, its in 1..2");
+    else if (blocksize <= 0 || blocksize % (2 * ops))  // io.py:52
+        rc = fail(s, PS_ERR_INVALID, "blocksize %d must be a multiple of 2*ops", blocksize);
+    else if (nx <= 0 || ny <= 0 || nx % blocksize || ny % blocksize)  // process.py:143
+        rc = fail(s, PS_ERR_INVALID, "array %dx%d not divisible by blocksize %d", nx, ny, blocksize);
+    else if ((size_t)3 * nv * nx * ny >= (size_t)1 << 31)
+        rc = fail(s, PS_ERR_UNSUPPORTED, "field too large for 32-bit offsets");
+    s->mpss = blocksize > 0 && ops > 0 ? blocksize / (2 * ops) - 1 : 0;
+    if (rc == PS_OK && s->mpss < 1)
+        rc = fail(s, PS_ERR_INVALID, "blocksize %d gives no swept level (MPSS < 1)", blocksize);
+    if (rc == PS_OK) {
+        s->hook = new HookModule();
+        s->hook->nv = nv;
+        s->hook->ops = ops;
+        s->hook->its = its;
+        s->hook_src = source;
+        // levels per half-cycle: MPSS, fewer where the hook's linear slots
+        // (one per level) would not fit in shared memory
+        s->H = s->mpss;
+        for (;;) {
+            s->chunk = (2 * ops * (s->H + 1) <= 32) ? 32 : 64;
+            const bool fits = 2 * ops * (s->H + 1) <= 64 && stream_smem(s) <= 227 * 1024 &&
+                              seam_smem(s) <= 227 * 1024;
+            if (fits || s->H == 1) break;
+            --s->H;
+        }
+        std::vector<char> cubin;
+        std::string log;
+        rc = hook_compile(hook_program(source, name ? name : "hook.cu", nv, ops, its), &cubin, &log);
+        if (rc) fail(s, PS_ERR_COMPILE, "step hook %s did not compile:\n%s", name ? name : "", log.c_str());
+        if (rc == PS_OK) rc = solver_open(s);  // device, stream (the primary context), bases
+        if (rc == PS_OK) {
+            std::string err;
+            if (hook_load(s->hook, cubin, &err)) rc = fail(s, PS_ERR_CUDA, "%s", err.c_str());
+        }
+    }
     if (rc != PS_OK) {
-        g_create_error = s->err;  // readable through ps_last_error(NULL)
+        g_create_error = s->err;
         ps_destroy(s);
         return rc;
     }
@@ -790,6 +1115,12 @@ int ps_destroy(ps_solver* s)
         if (r) cudaFree(r);
     if (s->xface) cudaFree(s->xface);
     if (s->yface) cudaFree(s->yface);
+    if (s->d_segs) cudaFree(s->d_segs);
+    if (s->d_ufirst) cudaFree(s->d_ufirst);
+    if (s->hook) {
+        if (s->hook->mod) drv().moduleUnload(s->hook->mod);
+        delete s->hook;
+    }
     for (auto& p : s->pending) {
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
@@ -811,6 +1142,23 @@ int ps_set_global(ps_solver* s, const char* name, const void* value, size_t nbyt
     if (!s || !name || !value) return PS_ERR_INVALID;
     if (nbytes != 1 && nbytes != 2 && nbytes != 4 && nbytes != 8)
         return fail(s, PS_ERR_INVALID, "constant %s: unsupported size %zu", name, nbytes);
+    if (s->hook) {
+        // the hook's own __constant__, in every kernel kind's copy, written in
+        // stream order (kernels queued before keep the old value)
+        PS_CUDA(s, cudaSetDevice(s->device));
+        HookConst* c = hook_const(s->hook, name);
+        if (!c) return fail(s, PS_ERR_INVALID, "the step hook declares no __constant__ %s", name);
+        unsigned char buf[8];
+        if (!hook_encode(value, nbytes, c->size, hook_const_kind(s->hook_src, name), buf))
+            return fail(s, PS_ERR_UNSUPPORTED, "constant %s: %zu-byte type", name, c->size);
+        for (int k = 0; k < 3; ++k) {
+            CUresult r = drv().memcpyHtoDAsync(c->ptr[k], buf, c->size, (CUstream)s->stream);
+            if (r != CUDA_SUCCESS)
+                return fail(s, PS_ERR_CUDA, "constant %s: %s", name, cu_error(r).c_str());
+        }
+        s->globals[name] = decode_value(value, nbytes);
+        return PS_OK;
+    }
     if (!find_global(s, name)) return fail(s, PS_ERR_INVALID, "no constant named %s", name);
     s->globals[name] = decode_value(value, nbytes);
     return PS_OK;
@@ -819,6 +1167,14 @@ int ps_set_global(ps_solver* s, const char* name, const void* value, size_t nbyt
 int ps_get_global(ps_solver* s, const char* name, void** handle, size_t* size)
 {
     if (!s || !name) return PS_ERR_INVALID;
+    if (s->hook) {
+        PS_CUDA(s, cudaSetDevice(s->device));
+        HookConst* c = hook_const(s->hook, name);
+        if (!c) return fail(s, PS_ERR_INVALID, "the step hook declares no __constant__ %s", name);
+        if (handle) *handle = (void*)c;  // `name` first, like the built-ins' GlobalSpec
+        if (size) *size = c->size;
+        return PS_OK;
+    }
     const GlobalSpec* g = find_global(s, name);
     if (!g) return fail(s, PS_ERR_INVALID, "no constant named %s", name);
     if (handle) *handle = (void*)g;
@@ -1051,6 +1407,11 @@ struct BatchInst {
     double* yface = nullptr;
     size_t yface_n = 0;  // elements of both y-face buffers
     bool have_state = false;
+    // levels advanced since this instance's state was set: the step function
+    // of the next level sees globalTimeStep = level + 1, as one solver run of
+    // all levels so far would show it (the reference starts at 1,
+    // pysweep/core/solver.py:162)
+    int64_t level = 0;
     std::map<std::string, double> globals;
 };
 
@@ -1074,6 +1435,8 @@ struct ps_batch {
     int graph_cur = -1;
     int64_t graph_launches = 0;
     int64_t launches = 0;
+    // the instances' level counters the device descriptors were uploaded with
+    std::vector<int64_t> desc_level;
     std::string err;
 };
 
@@ -1146,7 +1509,7 @@ int batch_upload(ps_batch* b)
             a.seg_units = b->fast ? I.ny / 32 : I.nseg;
             a.off = par ? b->bs / 2 : 0;  // prism bands alternate by half a block
             a.its = b->its;
-            a.gts_base = 0;
+            a.gts_base = (int)I.level;
             a.p = make_params_g(b->eq, I.globals);
             a.seam_direct = seam_direct(b->bs, b->ops, b->nv, b->its, b->H, sizeof(double)) ? 1 : 0;
         }
@@ -1155,7 +1518,19 @@ int batch_upload(ps_batch* b)
     PSB_CUDA(b, cudaMemcpyAsync(b->d_desc, d.data(), d.size() * sizeof(SweptArgs),
                                 cudaMemcpyHostToDevice, b->stream));
     PSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    b->desc_level.resize(n);
+    for (int i = 0; i < n; ++i) b->desc_level[i] = b->inst[i].level;
     return PS_OK;
+}
+
+// Whether the uploaded descriptors carry the instances' current level counters
+// (the captured graph reads the descriptors from device memory at every replay).
+bool batch_desc_current(const ps_batch* b)
+{
+    if (b->desc_level.size() != b->inst.size()) return false;
+    for (size_t i = 0; i < b->inst.size(); ++i)
+        if (b->desc_level[i] != b->inst[i].level) return false;
+    return true;
 }
 
 size_t batch_tile_smem(const ps_batch* b)
@@ -1462,6 +1837,7 @@ int ps_batch_set_state(ps_batch* b, int index, const double* src, int levels, in
                                     b->stream));
     if (!src_on_device) PSB_CUDA(b, cudaStreamSynchronize(b->stream));
     I.have_state = true;
+    I.level = 0;
     return PS_OK;
 }
 
@@ -1504,11 +1880,15 @@ int ps_batch_run(ps_batch* b, int64_t nlevels, int use_graph)
             b->graph_levels = nlevels;
             b->graph_cur = b->cur;
             b->graph_launches = n;
+        } else if (!batch_desc_current(b)) {
+            int rc = batch_upload(b);  // new level counters for the same graph
+            if (rc) return rc;
         }
         PSB_CUDA(b, cudaGraphLaunch(b->gexec, b->stream));
         b->launches += b->graph_launches;
     }
     b->cur ^= (int)(nhalf & 1);
+    for (auto& I : b->inst) I.level += nlevels;
     return PS_OK;
 }
 

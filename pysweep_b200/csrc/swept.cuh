@@ -37,8 +37,10 @@
 // per-cell function as the standard decomposition, so swept and standard
 // results are bit-identical.
 #pragma once
+#ifndef __CUDACC_RTC__  // run-time compilation (user step hooks) has no host headers
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 #include "equations.cuh"
 
@@ -68,6 +70,16 @@ struct SweptArgs {
     long long L0;  // global level index of this half-cycle's level 0
     int gts_base;  // the step function sees globalTimeStep = gts_base + level
     EqParams p;
+    // Optional table of column segments that need not divide the bands
+    // evenly (register streams): segment i = (band, first column, end
+    // column, the segment left of it in its band, cyclically); warp u of a
+    // stream launch runs segments ufirst[u] .. ufirst[u+1]-1, the seams run
+    // one CTA per segment.  nullptr: nseg equal segments per band, unit =
+    // band * nseg + segment.
+    const int4* __restrict__ segs;
+    const int* __restrict__ ufirst;
+    int nunits;  // stream warps with the table
+    int nsegs;   // segments with the table
 };
 
 __device__ __forceinline__ int wrap(int v, int n)
@@ -89,6 +101,22 @@ __device__ __forceinline__ int xface_col(int g, int m, int ny)
 __device__ __forceinline__ int seg_start(const SweptArgs& a, int s)
 {
     return a.seg_unit * (int)(((long long)s * a.seg_units) / a.nseg);
+}
+
+// Segment i: its band, columns [s0, s1) and the segment whose right edge
+// meets its left edge (for the seam at s0).
+struct SegGeom {
+    int band, s0, s1, left;
+};
+__device__ __forceinline__ SegGeom seg_geom(const SweptArgs& a, int i)
+{
+    if (a.segs) {
+        const int4 t = a.segs[i];
+        return SegGeom{t.x, t.y, t.z, t.w};
+    }
+    const int band = i / a.nseg, seg = i % a.nseg;
+    return SegGeom{band, seg_start(a, seg), seg_start(a, seg + 1),
+                   band * a.nseg + (seg + a.nseg - 1) % a.nseg};
 }
 
 // Global -> shared copies that complete asynchronously (cp.async; one
@@ -156,12 +184,14 @@ __host__ __device__ inline int seam_xoff(int ops, int nv, int m)
     // sum over levels 1..m-1 of nv * 2 * 2OPS * (2*OPS*m' + 2*2OPS)
     return nv * 4 * ops * (ops * m * (m - 1) + 4 * ops * (m - 1));
 }
-// Shared memory of one seam CTA in elements: its+1 tile slots, then the
+// Shared memory of one seam CTA in elements: nslot tile slots (its+1 for the
+// built-in equations' ring, hmax+2 for step hooks' linear slots), then the
 // staged faces of levels 1 .. hmax-1.
 __host__ __device__ inline size_t seam_smem_elems(bool gap, int bx, int ops, int nv, int its,
-                                                  int hmax)
+                                                  int hmax, int nslot = 0)
 {
-    const size_t slots = (size_t)(its + 1) * nv * bx * (2 * ops * (hmax + 1));
+    if (nslot == 0) nslot = its + 1;
+    const size_t slots = (size_t)nslot * nv * bx * (2 * ops * (hmax + 1));
     return slots + seam_yoff(gap, bx, ops, nv, hmax) + (gap ? seam_xoff(ops, nv, hmax) : 0);
 }
 
@@ -169,13 +199,14 @@ __host__ __device__ inline size_t seam_smem_elems(bool gap, int bx, int ops, int
 // two or fewer seam CTAs per SM and the bare tile slots fit more (large
 // Euler tiles; heat tiles keep seven with staging).
 __host__ __device__ inline bool seam_direct(int bx, int ops, int nv, int its, int hmax,
-                                            size_t esize)
+                                            size_t esize, int nslot = 0)
 {
+    if (nslot == 0) nslot = its + 1;
     const size_t cap = 227 * 1024;
-    const size_t ys = seam_smem_elems(false, bx, ops, nv, its, hmax);
-    const size_t gs = seam_smem_elems(true, bx, ops, nv, its, hmax);
+    const size_t ys = seam_smem_elems(false, bx, ops, nv, its, hmax, nslot);
+    const size_t gs = seam_smem_elems(true, bx, ops, nv, its, hmax, nslot);
     const size_t staged = esize * (ys > gs ? ys : gs);
-    const size_t bare = esize * (size_t)(its + 1) * nv * bx * (2 * ops * (hmax + 1));
+    const size_t bare = esize * (size_t)nslot * nv * bx * (2 * ops * (hmax + 1));
     return cap / staged <= 2 && cap / bare > cap / staged;
 }
 
@@ -187,6 +218,24 @@ __device__ __forceinline__ long long frame_slot(const SweptArgs& a, long long L)
     if (step % a.frame_every) return -1;
     long long s = step / a.frame_every - 1;
     return s < a.frame_cap ? s : -1;
+}
+
+// Shared-memory slot of level L in a stream or seam tile.  The built-in
+// equations use a ring of ITS+1 slots.  User step hooks address the previous
+// and next level as idx - TIMES and idx + TIMES (pysweep/equations/heat.cu:
+// 35-41), which needs the three levels at equal strides: LINEAR keeps level L
+// in slot L+1 (levels -1 and 0 first), i.e. Hmax+2 slots per tile.
+template <bool LINEAR, int ITS>
+__host__ __device__ __forceinline__ int slot_index(int L)
+{
+    if (LINEAR) return L + 1;
+    const int r = L % (ITS + 1);
+    return r < 0 ? r + ITS + 1 : r;
+}
+template <bool LINEAR, int ITS>
+__host__ __device__ __forceinline__ int slot_count(int hmax)
+{
+    return LINEAR ? hmax + 2 : ITS + 1;
 }
 
 // Equations whose functor evaluates a whole stream level at once (faces
@@ -203,16 +252,17 @@ struct FaceLevel<Eq, decltype((void)Eq::kFaceLevel)> {
 // ---------------------------------------------------------------- stream ----
 // One CTA = one (band, segment) block.  GAP = false: prism (UpPyramid);
 // GAP = true: gap (XBridge) centred on the band's upper boundary row.
-template <class Eq, int ITS, int W, bool GAP, int NT>
+template <class Eq, int ITS, int W, bool GAP, int NT, bool LINEAR = false>
 __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, double* sm)
 {
-    constexpr int OPS = Eq::OPS, O2 = 2 * OPS, RS = W + O2, NSLOT = ITS + 1;
+    constexpr int OPS = Eq::OPS, O2 = 2 * OPS, RS = W + O2;
     constexpr int RG = NT / W;  // row groups
     const int nv = a.nv, BX = a.bx, H = a.H, hx = a.hx, nx = a.nx, ny = a.ny;
     const int SL = nv * BX * RS;  // one level slot
     const int CS = nv * BX * O2;  // one carry
     double* slot = sm;
-    double* carry = sm + NSLOT * SL;
+    double* carry = sm + slot_count<LINEAR, ITS>(a.Hmax) * SL;
+    auto slot_at = [&](int L) { return slot + slot_index<LINEAR, ITS>(L) * SL; };
     const int band = unit / a.nseg, seg = unit % a.nseg;
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
     const int s0 = seg * a.wy;
@@ -235,7 +285,7 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
         // ---- level 0 and level -1 from the base --------------------------
         {
             const int lo0 = GAP ? hx - O2 : 0, hi0 = GAP ? hx + O2 : BX;
-            double* s0p = slot;  // slot of level 0
+            double* s0p = slot_at(0);  // slot of level 0
             const double* b0 = a.bin + (size_t)(ITS - 1) * nv * nx * ny;
             const int n0 = nv * (hi0 - lo0) * RC;
             // level 0 (and level -1) arrive by cp.async: every copy of a
@@ -248,7 +298,7 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
             }
             if (ITS >= 2) {
                 const int lo1 = GAP ? hx - OPS : OPS, hi1 = GAP ? hx + OPS : BX - OPS;
-                double* s1p = slot + (NSLOT - 1) * SL;  // slot of level -1
+                double* s1p = slot_at(-1);  // slot of level -1
                 const double* b1 = a.bin + (size_t)(ITS - 2) * nv * nx * ny;
                 const int n1 = nv * (hi1 - lo1) * Wc;
                 for (int e = tid; e < n1; e += NT) {
@@ -267,9 +317,9 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
             const int rlo = GAP ? hx - OPS * m : OPS * m;
             const int rhi = GAP ? hx + OPS * m : BX - OPS * m;
             const int klo = first ? O2 * (m + 1) : O2;
-            double* out = slot + (m % NSLOT) * SL;
-            const double* cur = slot + ((m - 1) % NSLOT) * SL;
-            const double* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
+            double* out = slot_at(m);
+            const double* cur = slot_at(m - 1);
+            const double* prv = slot_at(m - 2);
             const int gts = a.gts_base + (int)(a.L0 + m);
             // gap: the prisms' rows of level m that the next level reads go
             // into level m's slot by cp.async while the level is computed
@@ -382,7 +432,7 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
         }
         // carry out of level H, then free the slots for the next chunk
         if (!last) {
-            const double* cur = slot + (H % NSLOT) * SL;
+            const double* cur = slot_at(H);
             double* cout_ = carry + H * CS;
             for (int e = tid; e < CS; e += NT) {
                 const int j = e % O2, t = e / O2;
@@ -410,6 +460,9 @@ __device__ __forceinline__ int log2_ceil(int n)
     return n <= 1 ? 0 : 32 - __clz(n - 1);
 }
 
+// floor(log2(n)) for n >= 1, at compile time
+__host__ __device__ constexpr int log2_const(int n) { return n <= 1 ? 0 : 1 + log2_const(n / 2); }
+
 // f(r, c) for every (r, c) in [0, nr) x [0, nc), spread over NT threads:
 // c from the low bits of the thread index (a power-of-two group of at least
 // nc threads, at most NT), r strided by the number of groups.  Masks and
@@ -418,7 +471,7 @@ template <int NT, class F>
 __device__ __forceinline__ void for_2d(int nr, int nc, int tid, F&& f)
 {
     static_assert((NT & (NT - 1)) == 0, "NT is a power of two");
-    constexpr int kLogNT = 31 - __builtin_clz(NT);
+    constexpr int kLogNT = log2_const(NT);
     const int lg = min(log2_ceil(nc), kLogNT);
     const int cw = 1 << lg;
     const int c0 = tid & (cw - 1), rs = NT >> lg;
@@ -426,23 +479,25 @@ __device__ __forceinline__ void for_2d(int nr, int nc, int tid, F&& f)
         for (int r = tid >> lg; r < nr; r += rs) f(r, c);
 }
 
-template <class Eq, int ITS, bool GAP, int NT, class T = double>
+template <class Eq, int ITS, bool GAP, int NT, class T = double, bool LINEAR = false>
 __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T* sm)
 {
     const T* bin = reinterpret_cast<const T*>(a.bin);
     const T* yface = reinterpret_cast<const T*>(a.yface);
     T* xface = reinterpret_cast<T*>(a.xface);
-    constexpr int OPS = Eq::OPS, O2 = 2 * OPS, NSLOT = ITS + 1;
+    constexpr int OPS = Eq::OPS, O2 = 2 * OPS;
     const int nv = a.nv, BX = a.bx, H = a.H, hx = a.hx, nx = a.nx, ny = a.ny;
     const int KC = OPS * (a.Hmax + 1);
     const int TW = 2 * KC;
     const int SL = nv * BX * TW;
     T* slot = sm;
-    const int band = unit / a.nseg, seg = unit % a.nseg;
-    const int x0 = seg_start(a, seg);
+    auto slot_at = [&](int L) { return slot + slot_index<LINEAR, ITS>(L) * SL; };
+    const SegGeom sg = seg_geom(a, unit);
+    const int band = sg.band;
+    const int x0 = sg.s0;
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
-    const int ul = band * a.nseg + (seg + a.nseg - 1) % a.nseg;  // left stream unit
-    const int ur = unit;                                          // right stream unit
+    const int ul = sg.left;  // left stream segment
+    const int ur = unit;     // right stream segment
     const int bup = wrap(band - 1, a.nb);
     const int tid = threadIdx.x;
     const int HF = a.Hmax - 1;
@@ -471,13 +526,13 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
         for (int v = 0; v < nv; ++v)
             for_2d<NT>(hi0 - lo0, 2 * O2, tid, [&](int r, int c) {
                 const int i = lo0 + r, k = KC - O2 + c;
-                cp_async_elem(slot + (v * BX + i) * TW + k,
+                cp_async_elem(slot_at(0) + (v * BX + i) * TW + k,
                               b0 + ((size_t)v * nx + grow(i)) * ny + gcol(k));
             });
         if (ITS >= 2) {
             const int lo1 = GAP ? hx - OPS : OPS, hi1 = GAP ? hx + OPS : BX - OPS;
             const T* b1 = bin + (size_t)(ITS - 2) * nv * nx * ny;
-            T* s1p = slot + (NSLOT - 1) * SL;
+            T* s1p = slot_at(-1);
             for (int v = 0; v < nv; ++v)
                 for_2d<NT>(hi1 - lo1, O2, tid, [&](int r, int c) {
                     const int i = lo1 + r, k = KC - OPS + c;
@@ -489,7 +544,7 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
     // faces of levels 1 .. H-1, staged: per level the y-faces
     // [side][v][row][j] (left block's right edge, then right block's left
     // edge) and, in the gap, the prisms' rows around it [v][rr][column]
-    T* ystage = slot + NSLOT * SL;
+    T* ystage = slot + slot_count<LINEAR, ITS>(a.Hmax) * SL;
     T* xstage = ystage + seam_yoff(GAP, BX, OPS, nv, a.Hmax);
     const bool direct = a.seam_direct != 0;
     for (int m = 1; m <= (direct ? 0 : H - 1); ++m) {
@@ -529,9 +584,9 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
         const int rhi = GAP ? hx + OPS * m : BX - OPS * m;
         const int clo = KC - OPS * m, chi = KC + OPS * m;
         const int nr = rhi - rlo, nc = chi - clo;
-        T* out = slot + (m % NSLOT) * SL;
-        const T* cur = slot + ((m - 1) % NSLOT) * SL;
-        const T* prv = slot + ((m + NSLOT - 2) % NSLOT) * SL;
+        T* out = slot_at(m);
+        const T* cur = slot_at(m - 1);
+        const T* prv = slot_at(m - 2);
         const int gts = a.gts_base + (int)(a.L0 + m);
         // level m's faces go to cells of level m's slot that the level does
         // not compute (columns beside the bridge, rows around the gap), and

@@ -6,6 +6,7 @@ arrays are numpy ``float64``; device arrays may be given as torch CUDA tensors
 (their ``data_ptr`` is passed straight to the library).
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -28,16 +29,30 @@ def _torch_stream(device):
 DTYPES = {"float64": 0, "float32": 1}
 
 
+def is_hook(equation):
+    """Whether `equation` names a step hook (a .cu file) rather than a built-in."""
+    return equation not in EQ and str(equation).endswith(".cu")
+
+
 class Engine:
-    """dtype: "float64" (default) or "float32" (the reference's `dtype:
+    """equation: a built-in name (heat, euler, example, checker, half), or the
+    path of a plugin's .cu file whose ``__device__ step(shared_state, idx,
+    globalTimeStep)`` is compiled at run time (NVRTC, sm_100a), as the
+    reference's io.buildGPUSource builds it; ``hook_source`` passes the text
+    instead (equation then only labels it).
+
+    dtype: "float64" (default) or "float32" (the reference's `dtype:
     float32`: float32 fields, each level evaluated in float64 and rounded;
     heat with forward Euler only)."""
 
     def __init__(self, equation, nx, ny, nv=None, ops=None, its=1, blocksize=16, device=0,
-                 dtype="float64"):
-        if equation not in EQ:
-            raise ValueError(f"unknown equation {equation!r}; built-ins are {sorted(EQ)}")
+                 dtype="float64", hook_source=None):
+        hook = hook_source is not None or is_hook(equation)
+        if not hook and equation not in EQ:
+            raise ValueError(f"unknown equation {equation!r}; built-ins are {sorted(EQ)}, "
+                             "or the path of a step hook's .cu file")
         self.equation = equation
+        self.hook = hook
         self.nv = nv if nv is not None else DEFAULT_NV.get(equation, 1)
         self.ops = ops if ops is not None else DEFAULT_OPS.get(equation, 1)
         self.nx, self.ny, self.its, self.bs, self.device = nx, ny, its, blocksize, device
@@ -47,14 +62,25 @@ class Engine:
         self._h = ctypes.c_void_p()
         self._stream = None  # cudaStream_t set by set_stream (None: the solver's own)
         L = _lib.lib()
-        rc = L.ps_create_typed(ctypes.byref(self._h), device, EQ[equation], self.nv, nx, ny,
-                               self.ops, its, blocksize, DTYPES[self.dtype.name])
+        if hook:
+            if self.dtype != np.float64:
+                raise ValueError("step hooks run on float64 fields")
+            if hook_source is None:
+                with open(equation) as f:
+                    hook_source = f.read()
+            name = os.path.basename(str(equation))
+            rc = L.ps_create_hook(ctypes.byref(self._h), device, hook_source.encode(),
+                                  name.encode(), self.nv, nx, ny, self.ops, its, blocksize)
+        else:
+            rc = L.ps_create_typed(ctypes.byref(self._h), device, EQ[equation], self.nv, nx, ny,
+                                   self.ops, its, blocksize, DTYPES[self.dtype.name])
         _lib.check(rc, None)
         self.shape = (self.nv, nx, ny)
 
     # -- constants ---------------------------------------------------------
     def set_global(self, name, value):
-        """Set one plugin constant, typed like the value (float, int or bool)."""
+        """Set one plugin constant, typed like the value (float, int or bool);
+        a step hook's constant receives it converted to its declared type."""
         if isinstance(value, (bool, np.bool_)):
             buf, n = ctypes.c_uint8(int(value)), 1
         elif isinstance(value, (int, np.integer)):
@@ -223,6 +249,22 @@ class Engine:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def check_hook(source_or_path, nv=1, ops=1, its=1, name=None):
+    """Compile a step hook without a device; returns "" or raises PySweepError
+    with the compiler's log (the check io.buildGPUSource's SourceModule makes)."""
+    src = source_or_path
+    if str(source_or_path).endswith(".cu") and os.path.exists(str(source_or_path)):
+        name = name or os.path.basename(str(source_or_path))
+        with open(source_or_path) as f:
+            src = f.read()
+    log = ctypes.create_string_buffer(1 << 16)
+    rc = _lib.lib().ps_hook_check(src.encode(), (name or "hook.cu").encode(), nv, ops, its, log,
+                                  len(log))
+    if rc != _lib.PS_OK:
+        raise _lib.PySweepError(rc, log.value.decode())
+    return log.value.decode()
 
 
 def plugin_constants(equation, globals_):

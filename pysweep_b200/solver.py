@@ -23,7 +23,12 @@ and the ``cuda.memcpy_htod`` it uses set the device constants, exactly as
 with a PyCUDA SourceModule (pysweep/equations/heat.py:38-46).  The GPU hook
 (``gpu:``) names the step function: the file names of the reference's
 plugins (heat.cu, euler.cu, example.cu, checker.cu, half.cu) and the bare
-names select the built-in sm_100a kernels.
+names select the built-in sm_100a kernels (their arithmetic follows the numpy
+plugins operation by operation); any other ``.cu`` file, or any file at all
+with the extra yaml key ``compile_hook: true``, is compiled at run time with
+NVRTC for sm_100a, as io.buildGPUSource (io.py:146-155) builds it with
+PyCUDA, and its ``__device__ step`` runs inside the swept and standard
+kernels.
 
 Output: the reference's HDF5 layout (io.py:78-90): datasets ``blocksize``,
 ``share``, ``exid``, ``globals``, ``clocktime`` and ``data[t, v, x, y]``.
@@ -63,7 +68,10 @@ class SourceModuleShim:
         self.engine = None
 
     def get_global(self, name):
-        size = 4 if name == "SCHEME" else 8
+        if self.engine is not None and self.engine.hook:
+            _, size = self.engine.global_handle(name)  # the hook's declared size
+        else:
+            size = 4 if name == "SCHEME" else 8
         return GlobalRef(self, name), size
 
     def apply(self, engine):
@@ -121,6 +129,7 @@ class Solver:
         self.write_output = True
         self.device = 0
         self.tiling = {}
+        self.compile_hook = False
         if yamlFileName is not None:
             self.yamlFileName = yamlFileName
             self._read_yaml()
@@ -152,6 +161,7 @@ class Solver:
         self.output_every = int(get("output_every", 1))
         self.write_output = bool(get("write_output", True))
         self.tiling = get("tiling", {}) or {}
+        self.compile_hook = bool(get("compile_hook", False))
         if self.cpu:
             self.loadCPUModule()
 
@@ -185,11 +195,15 @@ class Solver:
                           "assignInitialConditionsFunction.")
 
     def equation(self):
+        """The built-in step function's name, or the path of the hook to compile."""
         name = os.path.splitext(os.path.basename(str(self.gpu)))[0]
-        if name not in BUILTIN:
-            raise NotImplementedError(
-                f"GPU hook {self.gpu!r}: built-in step functions are {BUILTIN}")
-        return name
+        if name in BUILTIN and not self.compile_hook:
+            return name
+        path = str(self.gpu)
+        if not os.path.isfile(path):
+            raise FileNotFoundError(
+                f"GPU hook {self.gpu!r}: not a file (built-in step functions are {BUILTIN})")
+        return path if path.endswith(".cu") else (path, "hook")
 
     def createTimeStepData(self):
         """pysweep/core/solver.py:113-128."""
@@ -223,16 +237,24 @@ class Solver:
         nv, nx, ny = ic.shape
         self.createTimeStepData()
         self.moments.append(time.time())
+        hook_src = None
+        if isinstance(eqn, tuple):  # a hook file without the .cu suffix
+            with open(eqn[0]) as f:
+                hook_src = f.read()
+            eqn = eqn[0]
         self.engine = Engine(eqn, nx, ny, nv=nv, ops=self.operating, its=self.intermediate,
-                             blocksize=self.blocksize[0], device=self.device, dtype=fdt.name)
+                             blocksize=self.blocksize[0], device=self.device, dtype=fdt.name,
+                             hook_source=hook_src)
         if self.tiling:
             self.engine.configure(**self.tiling)
         src = SourceModuleShim()
+        if self.engine.hook:
+            src.engine = self.engine  # sizes and values go straight to the hook's constants
         if isinstance(self.cpu, types.ModuleType) and hasattr(self.cpu, "set_globals"):
             self.cpu.set_globals(*self.globals, source_mod=src)
-            if not src.values:  # the plugin set only CPU globals
+            if not src.values and not self.engine.hook:  # the plugin set only CPU globals
                 src.values = plugin_constants(eqn, self.globals)
-        else:
+        elif not self.engine.hook:
             src.values = plugin_constants(eqn, self.globals)
         src.apply(self.engine)
         self.engine.set_state(ic)

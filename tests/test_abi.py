@@ -45,7 +45,7 @@ def test_plugin_constants_follow_set_globals():
 
 
 def test_package_exports_the_documented_names():
-    """The names INTEGRATION.md uses are importable from the package."""
+    """The names the integration notes use are importable from the package."""
     import pysweep_b200
     for name in ("Solver", "Engine", "Batch", "plugin_constants", "PySweepError"):
         assert hasattr(pysweep_b200, name), name

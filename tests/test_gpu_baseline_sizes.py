@@ -1,0 +1,109 @@
+"""GPU parity at the benchmark configurations' own sizes.
+
+The smaller parity cases pin every code path; these run the configurations
+the benchmark times, with their default tilings, against the oracle:
+
+* heat 8192^2 FP64, blocksize 32, the benchmark's seeded Fourier field and
+  its tiling (12 levels per half-cycle; the automatic segments: the grid's
+  columns in one equal share per stream warp slot, cut at band boundaries,
+  which at 148 SMs gives 2016 segments of uneven width, 8 per band rounded
+  up), 36 levels: swept == standard == oracle, bitwise;
+* the isentropic vortex at 1024^2, blocksize 32 (the reference's Euler test
+  case, pysweep/tests/tests.py:106-163), 10 steps: bitwise against the oracle
+  with x*x; one step within 1e-12 of the reference's own arithmetic, which
+  squares numpy float64 scalars through libm pow (one ulp off x*x in about
+  0.1% of cases).  Over more steps the pressure-ratio limiter's cut-offs
+  (euler.py:250-256: ratios above 1e6, NaN or negative become 0) turn such
+  one-ulp differences into different branches: the oracle's own pow and x*x
+  runs differ by 5e-7 after 3 steps and 7e-4 after 10 at this size, so no
+  implementation of either arithmetic can stay within 1e-12 of the other;
+* Euler 4096^2, blocksize 16 (the large Euler configuration), 3 steps.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+EULER_RTOL = 1e-12
+
+
+def _run(eqn, ic, g, its, bs, nlevels, mode):
+    from pysweep_b200 import Engine, plugin_constants
+    e = Engine(eqn, ic.shape[1], ic.shape[2], nv=ic.shape[0], its=its, blocksize=bs)
+    for k, v in plugin_constants(eqn, g).items():
+        e.set_global(k, v)
+    e.set_state(ic)
+    e.run(nlevels, mode=mode)
+    out = e.get_state()
+    tiling = e.tiling()
+    e.close()
+    return out, tiling
+
+
+def _balanced_segments_per_band(nb, per, slots):
+    """The register streams' automatic segments (build_seg_table): the grid's
+    32-column units, band after band, in equal shares per warp slot, each
+    share cut at band boundaries; segments per band, rounded up."""
+    total = nb * per
+    shares = max(1, min(slots, total // 2))
+    segs = 0
+    for u in range(shares):
+        p, p1 = total * u // shares, total * (u + 1) // shares
+        while p < p1:
+            p = min(p1, (p // per + 1) * per)
+            segs += 1
+    return -(-segs // nb)
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def test_heat_8192_benchmark_field_and_tiling():
+    import torch
+    from bench import fourier_field, heat_globals
+    n, bs, nl = 8192, 32, 36
+    ic = fourier_field(n, seed=0)
+    g = heat_globals(n, 5000)
+    sw, tiling = _run("heat", ic, g, 1, bs, nl, "swept")
+    assert tiling["h"] == 12
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert tiling["nseg"] == _balanced_segments_per_band(n // bs, n // 32, sms * 3 * 4)
+    st, _ = _run("heat", ic, g, 1, bs, nl, "standard")
+    assert np.array_equal(sw, st)
+    _, ref, _ = oracle.standard("heat", ic, g, 1, nl, nthreads=oracle.max_threads(), frames=False)
+    assert np.array_equal(sw, ref)
+
+
+def test_euler_vortex_1024_blocksize_32():
+    from pysweep_b200.equations.euler import analytical_array
+    n, bs, steps = 1024, 32, 10
+    dx = 10.0 / n
+    g = [0.0, steps * 0.1 * dx, 0.1 * dx, dx, dx, 1.4]
+    ic = analytical_array(n, n, 0.0)
+    sw, tiling = _run("euler", ic, g, 2, bs, 2 * steps, "swept")
+    st, _ = _run("euler", ic, g, 2, bs, 2 * steps, "standard")
+    assert np.array_equal(sw, st)
+    nt = oracle.max_threads()
+    _, mul, _ = oracle.standard("euler", ic, g, 2, 2 * steps, nthreads=nt, frames=False,
+                                euler_square="mul")
+    assert np.array_equal(sw, mul)
+    one, _ = _run("euler", ic, g, 2, bs, 2, "swept")
+    _, pw, _ = oracle.standard("euler", ic, g, 2, 2, nthreads=nt, frames=False)
+    assert _rel(one, pw) < EULER_RTOL
+
+
+def test_euler_4096_blocksize_16():
+    from bench import euler_field
+    n, bs, steps = 4096, 16, 3
+    dx = 10.0 / n
+    g = [0.0, steps * 0.1 * dx, 0.1 * dx, dx, dx, 1.4]
+    ic = euler_field(n)
+    sw, _ = _run("euler", ic, g, 2, bs, 2 * steps, "swept")
+    st, _ = _run("euler", ic, g, 2, bs, 2 * steps, "standard")
+    assert np.array_equal(sw, st)
+    _, mul, _ = oracle.standard("euler", ic, g, 2, 2 * steps, nthreads=oracle.max_threads(),
+                                frames=False, euler_square="mul")
+    assert np.array_equal(sw, mul)

@@ -14,10 +14,10 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(lib, d_in, d_out, n, bs, steps, g):
+def _noalloc(lib, d_in, d_out, n, bs, steps, g, ny=None, stream=None):
     err = ctypes.create_string_buffer(256)
     rc = lib.ps_heat_swept_noalloc(ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(d_out.data_ptr()),
-                                   n, n, bs, steps, g[5], g[2], g[3], None, err, 256)
+                                   n, ny or n, bs, steps, g[5], g[2], g[3], stream, err, 256)
     return rc, err.value.decode()
 
 
@@ -69,3 +69,43 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                    n, n, 32, 10, 1.0, 1e-8, 1.0 / n, None, err, 256)
     assert rc == -1
     assert b"scratch" in err.value
+
+
+@pytest.mark.parametrize("nx,ny,bs,steps", [
+    (2048, 2048, 32, 40),   # 27 segments over 64 column units: uneven segments
+    (512, 256, 32, 29),     # rectangular: rows and columns tiled differently
+    (256, 512, 16, 0),      # no steps: the output is a copy of the input
+])
+def test_noalloc_uneven_rectangular_and_empty_runs_on_a_side_stream(nx, ny, bs, steps):
+    """The same bitwise bar on the sizes the first test does not reach: the
+    segment rule's uneven segments, nx != ny, zero steps, and a call queued on
+    a stream other than the default one."""
+    import torch
+    from pysweep_b200 import _lib
+    lib = _lib.lib()
+    dx = 1.0 / nx
+    dt = 0.2 * dx * dx
+    g = [0.0, steps * dt, dt, dx, dx, 1.0, True]
+    ic = np.random.default_rng(nx + ny + bs).standard_normal((1, nx, ny))
+    d_in = torch.from_numpy(ic).cuda()
+    d_out = torch.full_like(d_in, float("nan"))
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    rc, msg = _noalloc(lib, d_in, d_out, nx, bs, steps, g, ny=ny, stream=side.cuda_stream)
+    assert rc == 0, msg
+    side.synchronize()
+    got = d_out.cpu().numpy()
+    ref = ic if steps == 0 else _allocating(ic, bs, steps, g)
+    assert np.array_equal(got, ref), f"differs by {np.nanmax(np.abs(got - ref))}"
+
+
+def test_noalloc_rejects_overlapping_fields():
+    import torch
+    from pysweep_b200 import _lib
+    lib = _lib.lib()
+    buf = torch.zeros((2, 128, 128), dtype=torch.float64, device="cuda")
+    err = ctypes.create_string_buffer(256)
+    half = ctypes.c_void_p(buf.data_ptr() + 64 * 128 * 8)  # starts inside the input field
+    rc = lib.ps_heat_swept_noalloc(ctypes.c_void_p(buf.data_ptr()), half, 128, 128, 32, 3, 1.0,
+                                   1e-6, 1.0 / 128, None, err, 256)
+    assert rc == -1 and b"overlap" in err.value
