@@ -520,27 +520,15 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
     }
 }
 
-// Warps of a stream launch: one per segment, or, with a segment table, one
-// per equal share of the grid's columns (its segments in turn).
-__host__ __device__ inline int stream_units(const SweptArgs& a)
-{
-    return a.segs ? a.nunits : a.nb * a.nseg;
-}
-
 template <int BX, bool GAP, class T = double>
 __global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs a)
 {
     extern __shared__ double sm[];
     const int warp = threadIdx.x >> 5;
     const int unit = blockIdx.x * kFastWarps + warp;
-    if (unit >= stream_units(a)) return;  // whole warp leaves together
-    double* carry = sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax);
-    if (!a.segs) {
-        heat_fast_body<BX, GAP, T>(a, seg_geom(a, unit), unit, carry);
-        return;
-    }
-    for (int i = a.ufirst[unit]; i < a.ufirst[unit + 1]; ++i)
-        heat_fast_body<BX, GAP, T>(a, seg_geom(a, i), i, carry);
+    if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
+    heat_fast_body<BX, GAP, T>(a, seg_geom(a, unit), unit,
+                               sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
 }  // namespace psb

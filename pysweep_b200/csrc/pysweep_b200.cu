@@ -97,12 +97,6 @@ struct ps_solver {
     // user step hook compiled at run time (ps_create_hook); nullptr for the
     // built-in equations
     HookModule* hook = nullptr;
-    // register streams in automatic tiling: the balanced segment table
-    // (build_seg_table); seg_table false = nseg equal segments per band
-    bool seg_table = false;
-    int4* d_segs = nullptr;
-    int* d_ufirst = nullptr;
-    int seg_total = 0, seg_units = 0;
     std::string hook_src;    // the hook's source (declared types of its constants)
     std::string launch_err;  // a driver-API launch failure, reported by check_launch
 };
@@ -254,7 +248,7 @@ void launch_fast(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
 {
     auto k = heat_stream_fast<BX, GAP, T>;
     allow_big_smem(k);
-    const int units = stream_units(a);
+    const int units = a.nb * a.nseg;
     k<<<(units + kFastWarps - 1) / kFastWarps, 32 * kFastWarps, smem, st>>>(a);
 }
 
@@ -370,61 +364,6 @@ int drain_profile(ps_solver* s)
     return PS_OK;
 }
 
-// Balanced segments for the register streams: the grid's 32-column units,
-// band after band, cut into `slots` equal shares, one per stream warp, each
-// share cut again at band boundaries into segments.  With equal segments per
-// band the warps number nb * nseg, which rarely fills the GPU's warp slots
-// (8192^2 at bs 32: 256 bands x 6 segments = 1536 warps for 1776 slots, and 7
-// segments would need a second wave); equal shares fill every slot with the
-// same work, for some 30% more segments (seams).  Segments are numbered band
-// after band, so each segment's left neighbour is the one before it, or the
-// band's last one.
-int build_seg_table(ps_solver* s, int slots)
-{
-    const int nb = s->nx / s->bs, per = s->ny / 32;
-    const long long T = (long long)nb * per;
-    // shares of at least two units (64 columns) where the grid is small
-    const int U = (int)std::max<long long>(1, std::min<long long>(slots, T / 2));
-    if (s->seg_table && s->seg_units == U) return PS_OK;
-    std::vector<int4> segs;
-    std::vector<int> ufirst(U + 1);
-    std::vector<int> band_first(nb, -1);
-    for (int u = 0; u < U; ++u) {
-        ufirst[u] = (int)segs.size();
-        long long p = T * u / U;
-        const long long p1 = T * (u + 1) / U;
-        while (p < p1) {
-            const int band = (int)(p / per);
-            const long long e = std::min<long long>(p1, (long long)(band + 1) * per);
-            if (band_first[band] < 0) band_first[band] = (int)segs.size();
-            segs.push_back(make_int4(band, (int)(p - (long long)band * per) * 32,
-                                     (int)(e - (long long)band * per) * 32, 0));
-            p = e;
-        }
-    }
-    ufirst[U] = (int)segs.size();
-    for (size_t i = 0; i < segs.size(); ++i) {
-        const int b = segs[i].x;
-        const size_t last = (b + 1 < nb ? (size_t)band_first[b + 1] : segs.size()) - 1;
-        segs[i].w = segs[i].y == 0 ? (int)last : (int)i - 1;
-    }
-    if (s->d_segs) cudaFree(s->d_segs);
-    if (s->d_ufirst) cudaFree(s->d_ufirst);
-    s->d_segs = nullptr;
-    s->d_ufirst = nullptr;
-    s->seg_table = false;
-    PS_CUDA(s, cudaMalloc(&s->d_segs, segs.size() * sizeof(int4)));
-    PS_CUDA(s, cudaMalloc(&s->d_ufirst, ufirst.size() * sizeof(int)));
-    PS_CUDA(s, cudaMemcpy(s->d_segs, segs.data(), segs.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    PS_CUDA(s, cudaMemcpy(s->d_ufirst, ufirst.data(), ufirst.size() * sizeof(int),
-                          cudaMemcpyHostToDevice));
-    s->seg_table = true;
-    s->seg_units = U;
-    s->seg_total = (int)segs.size();
-    s->nseg = (s->seg_total + nb - 1) / nb;  // reported: segments per band, rounded up
-    return PS_OK;
-}
-
 int ensure_swept_buffers(ps_solver* s)
 {
     const int O2 = 2 * s->ops;
@@ -432,9 +371,8 @@ int ensure_swept_buffers(ps_solver* s)
     const int HF = std::max(s->H - 1, 0);
     const size_t xn = (size_t)nb * HF * 2 * s->nv * O2 * s->ny;
     // two y-face buffers: prism -> y-bridge, gap -> octahedron (the y-bridge
-    // and the gap stream run at the same time), one pair of sides per segment
-    const size_t nsegs = s->seg_table ? (size_t)s->seg_total : (size_t)nb * s->nseg;
-    const size_t yn = 2 * nsegs * 2 * HF * s->nv * s->bs * O2;
+    // and the gap stream run at the same time)
+    const size_t yn = 2 * (size_t)nb * s->nseg * 2 * HF * s->nv * s->bs * O2;
     if (xn > s->xface_n) {
         if (s->xface) cudaFree(s->xface);
         s->xface = nullptr;
@@ -596,14 +534,15 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     if (!K.fast && std::min(s->chunk, s->ny / s->nseg) < O2 * (s->H + 1))
         return fail(s, PS_ERR_INVALID, "segment width %d narrower than 2*ops*(h+1) = %d",
                     s->ny / s->nseg, O2 * (s->H + 1));
-    if (!s->nseg_auto || !K.fast) s->seg_table = false;
     if (s->nseg_auto) {
         if (K.fast) {
-            // one warp per equal share of the columns: 3 CTAs of 4 warps per SM fit
+            // one warp per (band, segment); 3 CTAs of 4 warps per SM fit
             int sms = 148;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-            int rc2 = build_seg_table(s, sms * 3 * kFastWarps);
-            if (rc2) return rc2;
+            const int slots = sms * 3 * kFastWarps;
+            const int nb = s->nx / s->bs;
+            s->nseg = std::max(1, std::min(s->ny / kFastChunk, slots / nb));
+            s->nseg = std::max(1, std::min(s->nseg, s->ny / 32));
         } else {
             // one CTA per (band, segment): the most segments that divide ny
             // and keep four chunks (and 2*ops*(h+1) columns) each.  Shorter
@@ -652,16 +591,9 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
     a.gts_base = gts0 - 1;
     a.xface = s->xface;
     a.yface = s->yface;
-    if (s->seg_table) {
-        a.segs = s->d_segs;
-        a.ufirst = s->d_ufirst;
-        a.nunits = s->seg_units;
-        a.nsegs = s->seg_total;
-    }
     a.p = make_params(s);
     a.seam_direct = solver_seam_direct(s) ? 1 : 0;
-    // seam CTAs: one per segment
-    const int units = s->seg_table ? s->seg_total : a.nb * a.nseg;
+    const int units = a.nb * a.nseg;
     if (s->hook) {
         // the hook's tiles: stream slots of bs rows x (chunk + 2 OPS) columns
         // whose levels sit one slot + OPS apart (the chunk's parallelogram),
@@ -692,7 +624,7 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         double cP = 0, cY = 0, cG = 0, cO = 0;
         for (int m = 1; m <= H; ++m) {
             const double rp = s->bs - 2.0 * s->ops * m, rg = 2.0 * s->ops * m;
-            const double cm = 2.0 * s->ops * m * units / a.nb;  // seam columns of a band
+            const double cm = 2.0 * s->ops * m * s->nseg;  // seam columns of a band
             const double cs = (double)s->ny - cm;           // stream columns of a band
             cP += rp * cs;
             cY += rp * cm;
@@ -704,7 +636,9 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
                                   : stream_smem(s);
         // P, then Y on `stream` beside G on the side stream (G reads nothing
         // that Y writes: its valid cells depend on the prisms' faces only,
-        // and it writes its y-faces into the second buffer), then O
+        // and adjacent bands share their segment boundaries, so G's
+        // trapezoids avoid both bands' y-bridge diamonds; it writes its
+        // y-faces into the second buffer), then O
         SweptArgs ag = a;
         ag.yface = at(s, s->yface, s->yface_n / 2);
         if ((rc = timed_launch(s, 0, cP * u, [&] { K.P(a, units, psm, s->stream); }))) return rc;
@@ -1115,8 +1049,6 @@ int ps_destroy(ps_solver* s)
         if (r) cudaFree(r);
     if (s->xface) cudaFree(s->xface);
     if (s->yface) cudaFree(s->yface);
-    if (s->d_segs) cudaFree(s->d_segs);
-    if (s->d_ufirst) cudaFree(s->d_ufirst);
     if (s->hook) {
         if (s->hook->mod) drv().moduleUnload(s->hook->mod);
         delete s->hook;

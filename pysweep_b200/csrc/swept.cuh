@@ -70,16 +70,6 @@ struct SweptArgs {
     long long L0;  // global level index of this half-cycle's level 0
     int gts_base;  // the step function sees globalTimeStep = gts_base + level
     EqParams p;
-    // Optional table of column segments that need not divide the bands
-    // evenly (register streams): segment i = (band, first column, end
-    // column, the segment left of it in its band, cyclically); warp u of a
-    // stream launch runs segments ufirst[u] .. ufirst[u+1]-1, the seams run
-    // one CTA per segment.  nullptr: nseg equal segments per band, unit =
-    // band * nseg + segment.
-    const int4* __restrict__ segs;
-    const int* __restrict__ ufirst;
-    int nunits;  // stream warps with the table
-    int nsegs;   // segments with the table
 };
 
 __device__ __forceinline__ int wrap(int v, int n)
@@ -103,17 +93,13 @@ __device__ __forceinline__ int seg_start(const SweptArgs& a, int s)
     return a.seg_unit * (int)(((long long)s * a.seg_units) / a.nseg);
 }
 
-// Segment i: its band, columns [s0, s1) and the segment whose right edge
-// meets its left edge (for the seam at s0).
+// Unit i = band * nseg + segment: its band, columns [s0, s1) and the unit
+// whose right edge meets its left edge (for the seam at s0).
 struct SegGeom {
     int band, s0, s1, left;
 };
 __device__ __forceinline__ SegGeom seg_geom(const SweptArgs& a, int i)
 {
-    if (a.segs) {
-        const int4 t = a.segs[i];
-        return SegGeom{t.x, t.y, t.z, t.w};
-    }
     const int band = i / a.nseg, seg = i % a.nseg;
     return SegGeom{band, seg_start(a, seg), seg_start(a, seg + 1),
                    band * a.nseg + (seg + a.nseg - 1) % a.nseg};
