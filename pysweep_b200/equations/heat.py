@@ -1,8 +1,9 @@
-"""Heat equation plugin: constants and analytic solution.
+"""Heat equation plugin: constants, CPU step and analytic solution.
 
 Contract of pysweep/equations/heat.py:33-46 (set_globals: t0, tf, dt, dx, dy,
-alpha, scheme; device constants DT, DX, DY, ALPHA, SCHEME) and the decaying
-sine of heat.py:95-113.
+alpha, scheme; device constants DT, DX, DY, ALPHA, SCHEME), the CPU step of
+heat.py:21-64 (what the CPU rows of a run with share < 1 use) and the
+decaying sine of heat.py:95-113.
 """
 import numpy
 
@@ -22,6 +23,28 @@ def set_globals(*args, source_mod=None):
             cuda.memcpy_htod(ckey, numpy.float64(val))
         ckey, _ = source_mod.get_global("SCHEME")
         cuda.memcpy_htod(ckey, numpy.intc(scheme))
+
+
+def step(state, iidx, arrayTimeIndex, globalTimeStep):
+    """One level at the cells `iidx` ((x, y) pairs) of the 4-D state
+    [t, v, x, y]: level arrayTimeIndex + 1 from arrayTimeIndex (and, for the
+    second Runge-Kutta stage, arrayTimeIndex - 1), forward Euler or two-stage
+    Runge-Kutta by `scheme` (heat.py:21-31).  The cells are evaluated together
+    as arrays, each in the per-cell operation order of heat.py:48-64, so every
+    value equals the per-cell loop's; neighbours wrap around the state's x and
+    y extent."""
+    idx = numpy.asarray(iidx, dtype=numpy.intp).reshape(-1, 2)
+    x, y = idx[:, 0], idx[:, 1]
+    cur = state[arrayTimeIndex, 0]
+    nx, ny = cur.shape
+    c = cur[x, y]
+    dxx = courant * (cur[(x + 1) % nx, y] - 2 * c + cur[x - 1, y])
+    dyy = courant * (cur[x, (y + 1) % ny] - 2 * c + cur[x, y - 1])
+    if scheme:
+        state[arrayTimeIndex + 1, 0, x, y] = (dxx + dyy) + c
+    else:
+        coeff, back = (1, 1) if globalTimeStep % 2 == 0 else (0.5, 0)
+        state[arrayTimeIndex + 1, 0, x, y] = coeff * (dxx + dyy) + state[arrayTimeIndex - back, 0, x, y]
 
 
 def analytical(npx, npy, t, alpha=0.1):

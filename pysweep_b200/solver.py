@@ -11,11 +11,16 @@ step arithmetic is the reference's (solver.py:113-128): a swept run computes
 ``MPSS*(maxGlobalSweptStep+1)`` levels and stores ``timeSteps`` frames, a
 standard run stores ``timeSteps+1`` frames.
 
-What runs where: every row runs on the GPU through the CUDA swept (or
-standard) kernels.  ``share`` below 1 requested a CPU/GPU split in the
-reference; the computed values do not depend on the decomposition (the
-reference's own swept, standard and CPU paths agree bitwise), so the whole
-domain runs on the GPU and the effective share is recorded as 1.0.
+What runs where: with ``share`` 1 every row runs on the GPU through the CUDA
+swept (or standard) kernels.  With ``share`` below 1 the first
+ceil(share * nx / bs) block rows run on the GPU and the others on the host,
+stepped by the CPU plugin's own numpy ``step`` as the reference's CPU ranks
+step them, with the edge strips exchanged after every half-cycle
+(share.SplitSolver; the reference's MajorSplit, process.py:131-176); the
+effective share after that rounding is recorded.  A plugin without a numpy
+``step`` (or float32 fields, or a hook file without the .cu suffix) runs every
+row on the GPU, with a warning: the computed values do not depend on the
+split.
 
 The CPU plugin (``cpu:``) keeps its contract: its ``set_globals(*globals,
 source_mod=...)`` is called with a module object whose ``get_global(name)``
@@ -47,6 +52,7 @@ import numpy as np
 import yaml
 
 from .engine import Engine, plugin_constants
+from .share import SplitSolver
 
 BUILTIN = ("heat", "euler", "example", "checker", "half")
 NV = {"heat": 1, "half": 1, "euler": 4}
@@ -225,9 +231,6 @@ class Solver:
     # -- run ---------------------------------------------------------------
     def __call__(self, start=0, stop=-1):
         self.moments.append(time.time())
-        if self.share < 1:
-            warnings.warn(f"share={self.share}: all rows run on the GPU (results do not depend "
-                          "on the CPU/GPU split)")
         eqn = self.equation()
         # float32 fields (yaml `dtype: float32`) stay float32 on the device
         fdt = np.dtype(np.float32) if self.dtype == np.float32 else np.dtype(np.float64)
@@ -242,11 +245,27 @@ class Solver:
             with open(eqn[0]) as f:
                 hook_src = f.read()
             eqn = eqn[0]
-        self.engine = Engine(eqn, nx, ny, nv=nv, ops=self.operating, its=self.intermediate,
-                             blocksize=self.blocksize[0], device=self.device, dtype=fdt.name,
-                             hook_source=hook_src)
-        if self.tiling:
-            self.engine.configure(**self.tiling)
+        # share < 1: the first rows on the GPU, the rest stepped on the host by
+        # the CPU plugin's own `step` (pysweep/core/process.py:131-176)
+        split = None
+        has_step = isinstance(self.cpu, types.ModuleType) and hasattr(self.cpu, "step")
+        if self.share < 1 and not (has_step and fdt == np.float64 and hook_src is None):
+            warnings.warn(f"share={self.share}: the CPU plugin has no numpy step for float64 "
+                          "rows, so all rows run on the GPU (results do not depend on the split)")
+        elif self.share < 1:
+            split = SplitSolver(eqn, nx, ny, self.share, cpu_module=self.cpu, nv=nv,
+                                ops=self.operating, its=self.intermediate,
+                                blocksize=self.blocksize[0], device=self.device,
+                                h=self.tiling.get("h", 0), nseg=self.tiling.get("nseg", 0))
+        self.effective_share = split.share if split else 1.0
+        if split:
+            self.engine = split.gpu.eng
+        else:
+            self.engine = Engine(eqn, nx, ny, nv=nv, ops=self.operating, its=self.intermediate,
+                                 blocksize=self.blocksize[0], device=self.device,
+                                 dtype=fdt.name, hook_source=hook_src)
+            if self.tiling:
+                self.engine.configure(**self.tiling)
         src = SourceModuleShim()
         if self.engine.hook:
             src.engine = self.engine  # sizes and values go straight to the hook's constants
@@ -257,7 +276,7 @@ class Solver:
         elif not self.engine.hook:
             src.values = plugin_constants(eqn, self.globals)
         src.apply(self.engine)
-        self.engine.set_state(ic)
+        (split or self.engine).set_state(ic)
         self.moments.append(time.time())
         every = max(1, self.output_every)
         # frames beyond the initial condition at full steps 1..nframes-1
@@ -265,10 +284,13 @@ class Solver:
         frames = (np.empty((nkeep,) + ic.shape, dtype=fdt) if (self.write_output and nkeep)
                   else None)
         mode = "swept" if self.simulation else "standard"
-        self.engine.run(self.levels, mode=mode, frames=frames, frame_every=every)
+        if split:  # every cell's arithmetic is the same in either decomposition
+            split.run(self.levels, frames=frames, frame_every=every)
+        else:
+            self.engine.run(self.levels, mode=mode, frames=frames, frame_every=every)
         self.engine.synchronize()
         self.moments.append(time.time())
-        self.final = self.engine.get_state()
+        self.final = split.get_state() if split else self.engine.get_state()
         if frames is not None:
             self.data = np.concatenate([ic[None], frames])
         else:
@@ -276,14 +298,15 @@ class Solver:
         self.arrayShape = (self.nframes,) + ic.shape
         if self.write_output:
             self._write(self.data, self.moments[-1] - self.moments[0])
-        self.engine.close()
+        (split or self.engine).close()
         clock = self.moments[stop] - self.moments[start]
         _update_log(self, clock)
         if self.verbose:
             print(f"Done in {self.moments[-1] - self.moments[0]} seconds...")
 
     def _write(self, data, clocktime):
-        payload = {"blocksize": np.array([self.blocksize[0]]), "share": np.array([1.0]),
+        payload = {"blocksize": np.array([self.blocksize[0]]),
+                   "share": np.array([self.effective_share]),
                    "exid": np.array(self.exid), "globals": np.array(self.globals, dtype=float),
                    "clocktime": np.array([clocktime]), "data": data.astype(self.dtype)}
         try:
@@ -349,7 +372,8 @@ def _update_log(solver, clocktime, path="log.yaml"):
     """Append the run to ./log.yaml with the reference's keys (io.py:10-27)."""
     entry = {datetime.now().strftime("%m/%d/%Y-%H:%M:%S"): {
         "runtime": float(clocktime), "swept": bool(solver.simulation),
-        "blocksize": int(solver.blocksize[0]), "share": 1.0, "cpu": str(solver.cpuStr),
+        "blocksize": int(solver.blocksize[0]),
+        "share": float(getattr(solver, "effective_share", 1.0)), "cpu": str(solver.cpuStr),
         "array_shape": [int(x) for x in solver.arrayShape],
         "time_per_step": float(clocktime / max(solver.arrayShape[0] - 1, 1))}}
     prev = {}
