@@ -179,9 +179,10 @@ def fp64_roof(cells, ms, clk):
 
 
 def ncu_traffic(kind, n, bs, h):
-    """DRAM bytes per launch of one kernel kind (h levels per half-cycle),
-    measured by ncu at this grid size and committed as a profile summary;
-    None where no capture of this size exists."""
+    """DRAM bytes per launch of one kernel kind (h levels per half-cycle)
+    from the committed ncu profile summary (measured at this grid size, or
+    scaled from a smaller capture where its header says so); None where the
+    summary has no line for this size."""
     p = os.path.join(ROOT, "profiles", f"heat2d_swept_{kind}_traffic.txt")
     try:
         for line in open(p):
@@ -439,9 +440,54 @@ def run_b200(args):
     return 0
 
 
+def hook_line(args, n=4096, steps=600):
+    """A user step hook (tests/hooks/heat_numpy_order.cu: the heat plugin's
+    arithmetic in the reference's plugin format, compiled at run time) through
+    the swept and the standard decomposition, against the built-in heat
+    kernels on the same field."""
+    import torch
+
+    from pysweep_b200 import Engine, plugin_constants
+    hook = os.path.join(ROOT, "tests", "hooks", "heat_numpy_order.cu")
+    ic = fourier_field(n)
+    g = heat_globals(n, steps)
+    d_ic = torch.from_numpy(ic).cuda()
+    out, res = {}, {}
+    for label, eq, bs in (("hook", hook, 16), ("builtin", "heat", 32)):
+        e = Engine(eq, n, n, blocksize=bs)
+        for k, v in plugin_constants("heat", g).items():
+            e.set_global(k, v)
+        st = torch.cuda.Stream()
+        e.set_stream(st.cuda_stream)
+        for mode in ("swept", "standard"):
+            e.set_state(d_ic)
+            e.run(steps, mode=mode)
+            e.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(st)
+            e.set_state(d_ic)
+            e.run(steps, mode=mode)
+            ev1.record(st)
+            e.synchronize()
+            res[(label, mode)] = float(n) * n * steps / (ev0.elapsed_time(ev1) / 1000) / 1e9
+            out[(label, mode)] = e.get_state()
+        e.close()
+    return {"metric": "step hook Gcell-updates/s FP64 (heat in the plugin format, NVRTC)",
+            "unit": "Gcell-updates/s", "n": n, "time_steps": steps,
+            "hook_blocksize": 16, "builtin_blocksize": 32,
+            "hook_swept": res[("hook", "swept")], "hook_standard": res[("hook", "standard")],
+            "builtin_swept": res[("builtin", "swept")],
+            "builtin_standard": res[("builtin", "standard")],
+            "hook_equals_builtin": bool(np.array_equal(out[("hook", "swept")],
+                                                       out[("builtin", "swept")])),
+            "hook_swept_equals_standard": bool(np.array_equal(out[("hook", "swept")],
+                                                              out[("hook", "standard")]))}
+
+
 def secondary_lines(args):
     """The other targets of the metric, on the same GPU after the headline:
-    Euler swept vs standard (4096^2, blocksize 16, 1000 steps), the adjoint's
+    Euler swept vs standard (4096^2, blocksize 16, 1000 steps), a user step
+    hook compiled at run time against the built-in heat kernels, the adjoint's
     cost against its forward pass (2048^2, 2000 steps, 32 finite-difference
     directions) and the batched instances against one solver per instance
     (256 heat instances for 1000 steps; the 64 Euler instances for
@@ -456,6 +502,7 @@ def secondary_lines(args):
     quick = copy.copy(args)
     quick.steps, quick.warmup = 1, 1
     for name, fn in (("euler", lambda: euler_line(args)),
+                     ("hook", lambda: hook_line(args)),
                      ("adjoint", lambda: adjoint_line(args)),
                      ("batched", lambda: batched_line(quick, SECONDARY_EULER_BATCH_STEPS))):
         t0 = time.perf_counter()
