@@ -52,7 +52,7 @@ import numpy as np
 import yaml
 
 from .engine import Engine, plugin_constants
-from .share import SplitSolver
+from .share import SplitSolver, gpu_rows
 
 BUILTIN = ("heat", "euler", "example", "checker", "half")
 NV = {"heat": 1, "half": 1, "euler": 4}
@@ -252,7 +252,9 @@ class Solver:
         if self.share < 1 and not (has_step and fdt == np.float64 and hook_src is None):
             warnings.warn(f"share={self.share}: the CPU plugin has no numpy step for float64 "
                           "rows, so all rows run on the GPU (results do not depend on the split)")
-        elif self.share < 1:
+        elif self.share < 1 and gpu_rows(nx, self.blocksize[0], self.share) < nx:
+            # (when ceil(share * block rows) covers every block row, all rows
+            # run on the GPU, as in the reference)
             split = SplitSolver(eqn, nx, ny, self.share, cpu_module=self.cpu, nv=nv,
                                 ops=self.operating, its=self.intermediate,
                                 blocksize=self.blocksize[0], device=self.device,
