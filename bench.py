@@ -874,9 +874,30 @@ def adjoint_line(args):
         worst = max(worst, abs(d(h) - an) / max(abs(an), 1e-300))
         worst_r = max(worst_r, abs((4 * d(hr / 2) - d(hr)) / 3 - an) / max(abs(an), 1e-300))
     t_f, t_b = statistics.median(fwd), statistics.median(bwd)
+    # the same solve through the swept decomposition (SweptHeatVar): forward,
+    # and backward with each segment recomputed by the swept forward kernels
+    # and walked back by the swept adjoint kernels
+    for _ in range(args.warmup):
+        xu = u0.clone().requires_grad_(True)
+        xa = alpha0.clone().requires_grad_(True)
+        (0.5 * ((heat_solve(xu, xa, steps, dt, dx, every, swept=True) - target) ** 2).sum()).backward()
+    sfwd, sbwd = [], []
+    for _ in range(args.steps):
+        su = u0.clone().requires_grad_(True)
+        sa = alpha0.clone().requires_grad_(True)
+        t_sf, suT = timed(lambda: heat_solve(su, sa, steps, dt, dx, every, swept=True))
+        sloss = 0.5 * ((suT - target) ** 2).sum()
+        t_sb, _ = timed(lambda: sloss.backward())
+        sfwd.append(t_sf)
+        sbwd.append(t_sb)
+    t_sf, t_sb = statistics.median(sfwd), statistics.median(sbwd)
+    same = bool((su.grad == gu).all()) and bool((sa.grad == ga).all())
     return {
         "metric": "adjoint/forward cost", "value": t_b / t_f, "unit": "x", "higher_is_better": False,
         "forward_ms": t_f, "backward_ms": t_b, "n": n, "time_steps": steps, "checkpoint_every": every,
+        "swept": {"forward_ms": t_sf, "backward_ms": t_sb, "backward_over_swept_forward": t_sb / t_sf,
+                  "backward_over_fastest_forward": t_sb / min(t_f, t_sf),
+                  "gradients_equal_standard": same},
         "fd_directions": args.adj_dirs, "fd_h": h, "fd_max_rel_err": worst,
         "fd_richardson_h": hr, "fd_richardson_max_rel_err": worst_r, "dtype": "f64",
         "data": "synthetic", "steps": args.steps, "warmup": args.warmup}

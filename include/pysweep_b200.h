@@ -39,6 +39,12 @@ extern "C" {
 #define PS_EQ_EXAMPLE 2
 #define PS_EQ_CHECKER 3
 #define PS_EQ_HALF 4
+/* Heat with a courant number per cell (one variable) and its adjoint (two
+ * variables: lambda and the accumulated dJ/dC), the kernels of the
+ * differentiable solve (pysweep_b200.adjoint); their grid fields are set with
+ * ps_set_field. */
+#define PS_EQ_HEATVAR 6
+#define PS_EQ_HEATVAR_ADJ 7
 
 /* Storage type of a solver's fields (ps_create_typed).  PS_DTYPE_F32 is the
  * reference's `dtype: float32` (pysweep/core/io.py:72-73): every level is
@@ -181,6 +187,20 @@ int ps_set_state(ps_solver *s, const double *src, int levels, int src_on_device)
 int ps_run(ps_solver *s, int mode, int64_t nlevels, int gts0, double *frames, int64_t frame_cap,
            int frame_every, int frames_on_device);
 
+/*
+ * Grid fields of PS_EQ_HEATVAR and PS_EQ_HEATVAR_ADJ solvers ([nx][ny] device
+ * arrays the caller keeps alive while runs are queued).  index 0: courant
+ * numbers alpha*dt/dx^2 (both equations).  index 1: an array of
+ * [LEN][nx][ny] (LEN: the solver's constant of that name, ps_set_global); for
+ * PS_EQ_HEATVAR (NULL allowed) it receives, for every level gts a run
+ * computes, the old level's Laplacian at index gts-1; PS_EQ_HEATVAR_ADJ (a
+ * checkpoint segment of LEN steps, walked backward) reads the Laplacian of
+ * level gts at index LEN-gts.  ps_run refuses runs whose levels
+ * gts0 .. gts0+nlevels-1 fall outside 1 .. LEN.  No C-ABI counterpart in the
+ * reference (its solver has no adjoint).
+ */
+int ps_set_field(ps_solver *s, int index, double *d_field);
+
 /* Copy base level `level` (0 = newest, 1 = the one before) to dst.
  * Replaces the memcpy_dtoh after each phase group (functions.py:32). */
 int ps_get_state(ps_solver *s, double *dst, int level, int dst_on_device);
@@ -293,7 +313,13 @@ const char *ps_batch_last_error(const ps_batch *b);
  * adjoint steps lambda_n = lambda_{n+1} + L(C .* lambda_{n+1}),
  * dJ/dC += lambda_{n+1} .* L u_n run backward through it.  d_lamwork is a
  * scratch field.  `err` receives a message on failure.
+ *
+ * ps_heatvar_courant: only the courant field, d_courant = d_alpha*dt/dx/dx
+ * (the values ps_heatvar_forward writes), for the swept form of the same
+ * solve (PS_EQ_HEATVAR / PS_EQ_HEATVAR_ADJ solvers).
  */
+int ps_heatvar_courant(const double *d_alpha, double *d_courant, int nx, int ny, double dt,
+                       double dx, void *stream, char *err, size_t errlen);
 int ps_heatvar_forward(const double *d_u0, const double *d_alpha, double *d_uT, int nx, int ny,
                        int64_t nsteps, double dt, double dx, double *d_courant, double *d_work,
                        double *d_checkpoints, int every, void *stream, char *err, size_t errlen);

@@ -19,7 +19,8 @@ ERRORS = {
     -6: "hook compilation failed",
     -7: "call out of order",
 }
-EQ = {"heat": 0, "euler": 1, "example": 2, "checker": 3, "half": 4}
+EQ = {"heat": 0, "euler": 1, "example": 2, "checker": 3, "half": 4, "heatvar": 6,
+      "heatvar_adjoint": 7}
 MODE = {"swept": 0, "standard": 1}
 
 
@@ -44,6 +45,7 @@ _SIGS = {
     "ps_hook_check": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
     "ps_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "ps_set_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "ps_set_global": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p,
                                      ctypes.c_size_t]),
     "ps_get_global": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p,
@@ -74,6 +76,9 @@ _SIGS = {
                                        ctypes.POINTER(ctypes.c_double)]),
     "ps_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "ps_version": (ctypes.c_char_p, []),
+    "ps_heatvar_courant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "ps_heatvar_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int64,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_void_p,

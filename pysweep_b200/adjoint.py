@@ -28,19 +28,126 @@ def _call(fn, *args):
         raise _lib.PySweepError(rc, err.value.decode())
 
 
+class SweptHeatVar:
+    """The same solve through the swept decomposition (the engine's prism,
+    bridge and octahedron phases; Engine equations "heatvar" and
+    "heatvar_adjoint", csrc/equations.cuh HeatVar / HeatVarAdj):
+
+    * forward: u0 -> u_T with the courant field read by cell coordinates, the
+      state copied out every `every` steps (the checkpoints);
+    * backward: for the segments from the last to the first, the segment's
+      levels are recomputed from its checkpoint by the swept forward kernels,
+      which also store each old level's Laplacian L(u_n); then the adjoint
+      engine (state: lambda and dJ/dC) runs the segment backward through the
+      same decomposition, lambda_n = lambda_{n+1} + L(C lambda_{n+1}),
+      dJ/dC += lambda_{n+1} L(u_n).
+
+    Every cell sees the standard kernels' operations in the same order, so
+    u_T, lambda_0 and dJ/dalpha equal those of the standard solve bitwise.
+    The work runs on a stream of its own, ordered after the caller's current
+    stream on entry and before it on return."""
+
+    def __init__(self, nx, ny, every, blocksize=32, device=0):
+        from .engine import Engine
+        self.nx, self.ny, self.every, self.device = nx, ny, every, device
+        # one stream for both engines (the recompute's Laplacians are read by
+        # the adjoint engine's next run), ordered after the caller's stream
+        self.stream = torch.cuda.Stream(device=device)
+        self.fwd = Engine("heatvar", nx, ny, blocksize=blocksize, device=device)
+        self.adj = Engine("heatvar_adjoint", nx, ny, blocksize=blocksize, device=device)
+        for e in (self.fwd, self.adj):
+            e.set_stream(self.stream.cuda_stream)
+        self.lap = None
+
+    def _enter(self):
+        caller = torch.cuda.current_stream(self.device)
+        self.stream.wait_stream(caller)
+        return caller
+
+    def _leave(self, caller, *outs):
+        caller.wait_stream(self.stream)
+        for t in outs:
+            t.record_stream(caller)
+        return outs
+
+    def forward(self, u0, courant, nsteps, ck):
+        """u_T; ck[k] receives the state after k*every steps."""
+        caller = self._enter()
+        with torch.cuda.stream(self.stream):
+            f = self.fwd
+            f.set_field(0, courant)
+            f.set_field(1, None)
+            f.set_state(u0)
+            ck[0].copy_(u0)
+            done, k = 0, 0
+            while done < nsteps:
+                n = min(self.every, nsteps - done)
+                f.run(n)
+                done += n
+                k += 1
+                if done < nsteps:
+                    f.get_state(out=ck[k])
+            out = torch.empty_like(u0)
+            f.get_state(out=out)
+        return self._leave(caller, out)[0]
+
+    def backward(self, courant, ck, nsteps, lam_T):
+        """(lambda_0, dJ/dC)."""
+        nx, ny, every = self.nx, self.ny, self.every
+        caller = self._enter()
+        with torch.cuda.stream(self.stream):
+            if self.lap is None:
+                self.lap = torch.empty((every, nx, ny), dtype=lam_T.dtype, device=lam_T.device)
+            f, a = self.fwd, self.adj
+            f.set_field(0, courant)
+            f.set_field(1, self.lap)
+            f.set_global("LEN", every)
+            a.set_field(0, courant)
+            a.set_field(1, self.lap)
+            state = torch.zeros((2, nx, ny), dtype=lam_T.dtype, device=lam_T.device)
+            state[0].copy_(lam_T)
+            nseg = max(1, -(-nsteps // every))
+            for sidx in range(nseg - 1, -1, -1):
+                n0 = sidx * every
+                length = min(n0 + every, nsteps) - n0
+                if length <= 0:
+                    continue
+                f.set_state(ck[sidx])
+                f.run(length)          # u_{n0+1..} and L(u_{n0..n0+length-1})
+                a.set_global("LEN", length)
+                a.set_state(state)
+                a.run(length)          # lambda_{n0+length} -> lambda_{n0}
+                a.get_state(out=state)
+            f.set_field(1, None)
+            lam0, gC = state[0].clone(), state[1].clone()
+        return self._leave(caller, lam0, gC)
+
+    def close(self):
+        self.fwd.close()
+        self.adj.close()
+
+
 class HeatVarSolve(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, u0, alpha, nsteps, dt, dx, every):
+    def forward(ctx, u0, alpha, nsteps, dt, dx, every, swept=False):
         u0 = u0.contiguous()
         alpha = alpha.contiguous()
         nx, ny = u0.shape
         nseg = max(1, -(-nsteps // every))
-        courant = torch.empty_like(u0)
-        work = torch.empty_like(u0)
         ck = torch.empty((nseg, nx, ny), dtype=u0.dtype, device=u0.device)
-        uT = torch.empty_like(u0)
-        _call(_lib.lib().ps_heatvar_forward, _p(u0), _p(alpha), _p(uT), nx, ny, nsteps, dt, dx,
-              _p(courant), _p(work), _p(ck), every)
+        if swept:
+            courant = torch.empty_like(u0)
+            _call(_lib.lib().ps_heatvar_courant, _p(alpha), _p(courant), nx, ny, dt, dx)
+            sw = SweptHeatVar(nx, ny, every, device=u0.device.index or 0)
+            uT = sw.forward(u0, courant, nsteps, ck)
+            ctx.sw = sw
+        else:
+            courant = torch.empty_like(u0)
+            work = torch.empty_like(u0)
+            uT = torch.empty_like(u0)
+            _call(_lib.lib().ps_heatvar_forward, _p(u0), _p(alpha), _p(uT), nx, ny, nsteps, dt,
+                  dx, _p(courant), _p(work), _p(ck), every)
+            ctx.sw = None
         ctx.save_for_backward(courant, ck)
         ctx.cfg = (nsteps, dt, dx, every, nx, ny)
         return uT
@@ -50,17 +157,27 @@ class HeatVarSolve(torch.autograd.Function):
         courant, ck = ctx.saved_tensors
         nsteps, dt, dx, every, nx, ny = ctx.cfg
         g = grad_uT.contiguous()
+        if ctx.sw is not None:
+            lam0, gC = ctx.sw.backward(courant, ck, nsteps, g)
+            ctx.sw.close()
+            ctx.sw = None
+            # dJ/dalpha = dJ/dC * dt/dx/dx (scale_kernel's factor)
+            return lam0, gC * (dt / dx / dx), None, None, None, None, None
         states = torch.empty((every, nx, ny), dtype=g.dtype, device=g.device)
         lamwork = torch.empty_like(g)
         lam0 = torch.empty_like(g)
         galpha = torch.empty_like(g)
         _call(_lib.lib().ps_heatvar_adjoint, _p(courant), _p(ck), every, _p(g), _p(lam0),
               _p(galpha), nx, ny, nsteps, dt, dx, _p(states), _p(lamwork))
-        return lam0, galpha, None, None, None, None
+        return lam0, galpha, None, None, None, None, None
 
 
-def heat_solve(u0, alpha, nsteps, dt, dx, every=64):
-    return HeatVarSolve.apply(u0, alpha, int(nsteps), float(dt), float(dx), int(every))
+def heat_solve(u0, alpha, nsteps, dt, dx, every=64, swept=False):
+    """swept=False: the fused standard kernels (two levels per launch);
+    swept=True: the swept decomposition (SweptHeatVar).  Both give the same
+    values bitwise."""
+    return HeatVarSolve.apply(u0, alpha, int(nsteps), float(dt), float(dx), int(every),
+                              bool(swept))
 
 
 def heat_solve_reference(u0, alpha, nsteps, dt, dx):

@@ -522,6 +522,20 @@ int adj_cuda(cudaError_t e, char* err, size_t errlen)
 }
 }  // namespace
 
+extern "C" int ps_heatvar_courant(const double* d_alpha, double* d_courant, int nx, int ny,
+                                  double dt, double dx, void* stream, char* err, size_t errlen)
+{
+    int rc = adj_check(nx, ny, err, errlen);
+    if (rc) return rc;
+    if (!d_alpha || !d_courant) {
+        if (err && errlen) snprintf(err, errlen, "bad arguments");
+        return PS_ERR_INVALID;
+    }
+    courant_kernel<<<1024, 256, 0, (cudaStream_t)stream>>>(d_alpha, d_courant, (size_t)nx * ny, dt,
+                                                          dx);
+    return adj_cuda(cudaGetLastError(), err, errlen);
+}
+
 extern "C" int ps_heatvar_forward(const double* d_u0, const double* d_alpha, double* d_uT, int nx,
                                   int ny, int64_t nsteps, double dt, double dx, double* d_courant,
                                   double* d_work, double* d_checkpoints, int every, void* stream,

@@ -29,6 +29,11 @@ namespace psb {
 struct EqParams {
     double d[8];
     int i[4];
+    // grid fields read (and written) by equations that address cells by their
+    // coordinates (variable diffusivity and its adjoint); fs = elements of one
+    // level of f[1]
+    double* f[2];
+    long long fs;
 };
 
 // Element offsets of the points at distance k-2 along x (rows) and y (columns).
@@ -38,7 +43,26 @@ struct Nbr {
     int vs;  // variable stride
 };
 
-enum EqId { EQ_HEAT = 0, EQ_EULER = 1, EQ_EXAMPLE = 2, EQ_CHECKER = 3, EQ_HALF = 4 };
+enum EqId {
+    EQ_HEAT = 0,
+    EQ_EULER = 1,
+    EQ_EXAMPLE = 2,
+    EQ_CHECKER = 3,
+    EQ_HALF = 4,
+    EQ_HEATVAR = 6,
+    EQ_HEATVAR_ADJ = 7
+};
+
+// Equations whose step needs the cell's grid coordinates (Eq::kCoords and
+// Eq::step_at(..., row, col)) instead of the tile pointers alone.
+template <class Eq, class = void>
+struct Coords {
+    static constexpr bool value = false;
+};
+template <class Eq>
+struct Coords<Eq, decltype((void)Eq::kCoords)> {
+    static constexpr bool value = Eq::kCoords;
+};
 
 // heat.py: d[0] = courant = alpha*dt/dx/dx, i[0] = scheme (1 forward Euler, 0 RK2)
 struct Heat {
@@ -386,6 +410,72 @@ struct Euler {
 // tile leaves no room for the face scratch)
 struct EulerCell : Euler {
     static constexpr bool kFaceLevel = false;
+};
+
+// Heat with a courant number per cell, C = f[0][row][col] (the
+// differentiable solve's forward step, heatvar_step in adjoint.cu):
+//     u' = (C*((u[x+1]-2u)+u[x-1]) + C*((u[y+1]-2u)+u[y-1])) + u,
+// the heat plugin's order (pysweep/equations/heat.py:60-64) with the courant
+// number per cell.  With f[1] set, the step also stores the old level's
+// Laplacian ((u[x+1]-2u)+u[x-1]) + ((u[y+1]-2u)+u[y-1]) at
+// f[1][(gts-1)*fs + row*ny + col]: the recompute of one checkpoint segment for
+// the adjoint.  i[1] = nx, i[2] = ny.
+struct HeatVar {
+    static constexpr int OPS = 1;
+    static constexpr int ID = EQ_HEATVAR;
+    static constexpr bool kCoords = true;
+    __device__ static __forceinline__ void step_at(const double* __restrict__ u,
+                                                   const double* __restrict__, double* __restrict__ o,
+                                                   const Nbr& n, int gts, int, const EqParams& p,
+                                                   int row, int col)
+    {
+        const size_t at = (size_t)row * p.i[2] + col;
+        const double c = u[0];
+        const double C = __ldg(p.f[0] + at);
+        const double rx = __dadd_rn(__fma_rn(-2.0, c, u[n.x[3]]), u[n.x[1]]);
+        const double ry = __dadd_rn(__fma_rn(-2.0, c, u[n.y[3]]), u[n.y[1]]);
+        o[0] = __dadd_rn(__dadd_rn(__dmul_rn(C, rx), __dmul_rn(C, ry)), c);
+        if (p.f[1]) p.f[1][(size_t)(gts - 1) * p.fs + at] = __dadd_rn(rx, ry);
+    }
+};
+
+// The adjoint of HeatVar (heatvar_adjoint in adjoint.cu), run backward in
+// time through one checkpoint segment of i[3] steps.  Variable 0 is lambda,
+// variable 1 the accumulated dJ/dC.  Level gts (1-based in the segment) takes
+// lambda_{n+1} to
+//     lambda_n = lambda_{n+1} + L(C .* lambda_{n+1})
+// (L the periodic 5-point Laplacian in the order above, C .* lambda formed at
+// each of the five cells) and adds lambda_{n+1} * L(u_n) to dJ/dC in one fused
+// multiply-add, n = segment end - gts, L(u_n) from the segment's recompute at
+// f[1][(i[3]-gts)*fs + row*ny + col].  Each cell's levels are evaluated in
+// order in every decomposition, so dJ/dC sums in the same order as the
+// standard adjoint kernels.  i[1] = nx, i[2] = ny.
+struct HeatVarAdj {
+    static constexpr int OPS = 1;
+    static constexpr int ID = EQ_HEATVAR_ADJ;
+    static constexpr bool kCoords = true;
+    __device__ static __forceinline__ void step_at(const double* __restrict__ u,
+                                                   const double* __restrict__, double* __restrict__ o,
+                                                   const Nbr& n, int gts, int, const EqParams& p,
+                                                   int row, int col)
+    {
+        const int nx = p.i[1], ny = p.i[2];
+        const double* C = p.f[0];
+        const int rm = row == 0 ? nx - 1 : row - 1, rp = row + 1 == nx ? 0 : row + 1;
+        const int cm = col == 0 ? ny - 1 : col - 1, cp = col + 1 == ny ? 0 : col + 1;
+        const size_t at = (size_t)row * ny + col;
+        const double l = u[0];
+        const double mc = __dmul_rn(__ldg(C + at), l);
+        const double mxp = __dmul_rn(__ldg(C + (size_t)rp * ny + col), u[n.x[3]]);
+        const double mxm = __dmul_rn(__ldg(C + (size_t)rm * ny + col), u[n.x[1]]);
+        const double myp = __dmul_rn(__ldg(C + (size_t)row * ny + cp), u[n.y[3]]);
+        const double mym = __dmul_rn(__ldg(C + (size_t)row * ny + cm), u[n.y[1]]);
+        const double lm = __dadd_rn(__dadd_rn(__fma_rn(-2.0, mc, mxp), mxm),
+                                    __dadd_rn(__fma_rn(-2.0, mc, myp), mym));
+        o[0] = __dadd_rn(l, lm);
+        const double lu = __ldg(p.f[1] + (size_t)(p.i[3] - gts) * p.fs + at);
+        o[n.vs] = __fma_rn(l, lu, u[n.vs]);
+    }
 };
 
 }  // namespace psb

@@ -47,7 +47,10 @@ __global__ void __launch_bounds__(256) standard_kernel(const double* __restrict_
         n.y[k] = yy - y;
     }
     const size_t c = (size_t)x * ny + y;
-    Eq::step(cur + c, prev + c, out + c, n, gts, nv, p);
+    if constexpr (Coords<Eq>::value)
+        Eq::step_at(cur + c, prev + c, out + c, n, gts, nv, p, x, y);
+    else
+        Eq::step(cur + c, prev + c, out + c, n, gts, nv, p);
     if (frame) {
         for (int v = 0; v < nv; ++v) frame[c + (size_t)v * n.vs] = out[c + (size_t)v * n.vs];
     }
@@ -66,6 +69,9 @@ struct ps_solver {
     size_t esize = sizeof(double);  // bytes per element of every field and face buffer
     // tiling
     int H = 0, nseg = 1, chunk = 32, threads = 128;
+    // heatvar / heatvar adjoint: courant numbers, the segment's recomputed
+    // Laplacians (ps_set_field; device memory the caller owns)
+    double* field[2] = {nullptr, nullptr};
     bool nseg_auto = true;  // choose the segment count per run until configured
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -162,6 +168,8 @@ int eq_ops(int eq, int ops)
     switch (eq) {
     case PS_EQ_HEAT: return 1;
     case PS_EQ_HALF: return 1;
+    case PS_EQ_HEATVAR: return 1;
+    case PS_EQ_HEATVAR_ADJ: return 1;
     case PS_EQ_EULER: return 2;
     default: return ops;  // example / checker take the configured ops
     }
@@ -200,7 +208,20 @@ EqParams make_params_g(int eq, const std::map<std::string, double>& globals)
     return p;
 }
 
-EqParams make_params(const ps_solver* s) { return make_params_g(s->eq, s->globals); }
+EqParams make_params(const ps_solver* s)
+{
+    EqParams p = make_params_g(s->eq, s->globals);
+    if (s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJ) {
+        p.i[1] = s->nx;
+        p.i[2] = s->ny;
+        auto it = s->globals.find("LEN");
+        p.i[3] = it == s->globals.end() ? 0 : (int)it->second;
+        p.f[0] = s->field[0];
+        p.f[1] = s->field[1];
+        p.fs = (long long)s->nx * s->ny;
+    }
+    return p;
+}
 
 // Equation id of solvers running a user step hook (internal: ps_create_hook)
 constexpr int PS_EQ_HOOK = 5;
@@ -286,6 +307,10 @@ bool pick_swept(int eq, int ops, int its, int chunk, SweptSet* out)
     PS_SET(PS_EQ_CHECKER, 1, 2, 32, CheckerT<1>)
     PS_SET(PS_EQ_CHECKER, 2, 1, 32, CheckerT<2>)
     PS_SET(PS_EQ_CHECKER, 2, 2, 32, CheckerT<2>)
+    PS_SET(PS_EQ_HEATVAR, 1, 1, 32, HeatVar)
+    PS_SET(PS_EQ_HEATVAR, 1, 1, 64, HeatVar)
+    PS_SET(PS_EQ_HEATVAR_ADJ, 1, 1, 32, HeatVarAdj)
+    PS_SET(PS_EQ_HEATVAR_ADJ, 1, 1, 64, HeatVarAdj)
 #undef PS_SET
     return false;
 }
@@ -298,6 +323,8 @@ StdLaunch pick_standard(int eq, int ops)
     case PS_EQ_HALF: return launch_standard<Half>;
     case PS_EQ_EXAMPLE: return ops == 2 ? launch_standard<ExampleT<2>> : launch_standard<ExampleT<1>>;
     case PS_EQ_CHECKER: return ops == 2 ? launch_standard<CheckerT<2>> : launch_standard<CheckerT<1>>;
+    case PS_EQ_HEATVAR: return launch_standard<HeatVar>;
+    case PS_EQ_HEATVAR_ADJ: return launch_standard<HeatVarAdj>;
     default: return nullptr;
     }
 }
@@ -753,7 +780,7 @@ const GlobalSpec kGlobals[] = {
     {"DT", 0x1f},    {"DX", 0x1f},      {"DY", 0x1f},   {"ALPHA", 1 << PS_EQ_HEAT},
     {"SCHEME", (1 << PS_EQ_HEAT) | (1 << PS_EQ_EXAMPLE) | (1 << PS_EQ_CHECKER)},
     {"GAMMA", 1 << PS_EQ_EULER}, {"GAM_M1", 1 << PS_EQ_EULER}, {"DTDX", 1 << PS_EQ_EULER},
-    {"DTDY", 1 << PS_EQ_EULER},
+    {"DTDY", 1 << PS_EQ_EULER}, {"LEN", (1 << PS_EQ_HEATVAR) | (1 << PS_EQ_HEATVAR_ADJ)},
 };
 
 const GlobalSpec* find_global(const ps_solver* s, const char* name)
@@ -876,7 +903,8 @@ int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, i
 {
     if (!out) return PS_ERR_INVALID;
     *out = nullptr;
-    if (equation < PS_EQ_HEAT || equation > PS_EQ_HALF) return PS_ERR_INVALID;
+    if (equation < PS_EQ_HEAT || equation > PS_EQ_HEATVAR_ADJ || equation == PS_EQ_HOOK)
+        return PS_ERR_INVALID;
     if (dtype != PS_DTYPE_F64 && dtype != PS_DTYPE_F32) return PS_ERR_INVALID;
     ps_solver* s = new ps_solver();
     s->dtype = dtype;
@@ -893,6 +921,10 @@ int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, i
     if (equation == PS_EQ_HEAT || equation == PS_EQ_HALF) {
         if (nv != 1) rc = fail(s, PS_ERR_INVALID, "heat/half have one variable, got nv=%d", nv);
     }
+    if ((equation == PS_EQ_HEATVAR && nv != 1) || (equation == PS_EQ_HEATVAR_ADJ && nv != 2) ||
+        ((equation == PS_EQ_HEATVAR || equation == PS_EQ_HEATVAR_ADJ) && its != 1))
+        rc = fail(s, PS_ERR_INVALID, "heatvar has nv=1, its=1; its adjoint nv=2, its=1 (got nv=%d its=%d)",
+                  nv, its);
     if (equation == PS_EQ_EULER && (nv != 4 || its != 2))
         rc = fail(s, PS_ERR_INVALID, "euler needs nv=4 and its=2 (got nv=%d its=%d)", nv, its);
     if (ops != s->ops) rc = fail(s, PS_ERR_INVALID, "equation %d has ops=%d, got %d", equation, s->ops, ops);
@@ -1197,6 +1229,16 @@ int ps_set_state(ps_solver* s, const double* src, int levels, int src_on_device)
     return PS_OK;
 }
 
+int ps_set_field(ps_solver* s, int index, double* d_field)
+{
+    if (!s) return PS_ERR_INVALID;
+    if (s->eq != PS_EQ_HEATVAR && s->eq != PS_EQ_HEATVAR_ADJ)
+        return fail(s, PS_ERR_INVALID, "equation %d reads no grid fields", s->eq);
+    if (index < 0 || index > 1) return fail(s, PS_ERR_INVALID, "field index %d not 0 or 1", index);
+    s->field[index] = d_field;
+    return PS_OK;
+}
+
 int ps_run(ps_solver* s, int mode, int64_t nlevels, int gts0, double* frames, int64_t frame_cap,
            int frame_every, int frames_on_device)
 {
@@ -1204,6 +1246,18 @@ int ps_run(ps_solver* s, int mode, int64_t nlevels, int gts0, double* frames, in
     if (!s->have_state) return fail(s, PS_ERR_STATE, "ps_run before ps_set_state");
     if (nlevels < 0) return fail(s, PS_ERR_INVALID, "negative level count");
     if (frame_every < 0) return fail(s, PS_ERR_INVALID, "negative frame_every");
+    if ((s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJ) && !s->field[0])
+        return fail(s, PS_ERR_STATE, "heatvar: no courant field (ps_set_field 0)");
+    if (s->eq == PS_EQ_HEATVAR_ADJ && !s->field[1])
+        return fail(s, PS_ERR_STATE, "heatvar adjoint: no recomputed Laplacians (ps_set_field 1)");
+    if ((s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJ) && s->field[1] && nlevels > 0) {
+        // field 1 holds LEN levels: the run's levels gts0 .. gts0+nlevels-1 must index them
+        auto it = s->globals.find("LEN");
+        const int64_t len = it == s->globals.end() ? 0 : (int64_t)it->second;
+        if (gts0 < 1 || gts0 - 1 + nlevels > len)
+            return fail(s, PS_ERR_INVALID, "levels %d..%lld outside the %lld levels of field 1 (LEN)",
+                        gts0, (long long)(gts0 - 1 + nlevels), (long long)len);
+    }
     PS_CUDA(s, cudaSetDevice(s->device));
     double* dframes = frames;
     const size_t fe = field_elems(s);

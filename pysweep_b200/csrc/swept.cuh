@@ -251,6 +251,7 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
     auto slot_at = [&](int L) { return slot + slot_index<LINEAR, ITS>(L) * SL; };
     const int band = unit / a.nseg, seg = unit % a.nseg;
     const int r0 = GAP ? (a.off + band * BX - hx) : (a.off + band * BX);
+    const int r0w = wrap(r0, nx);
     const int s0 = seg * a.wy;
     const int tid = threadIdx.x;
     const int tk = tid % W, tr = tid / W;
@@ -337,9 +338,21 @@ __device__ __forceinline__ void stream_body(const SweptArgs& a, const int unit, 
             } else {
                 const int k = O2 + tk;
                 if (k >= klo && k < RC) {
+                    // grid column of tile column k at level m (equations that
+                    // address the grid by coordinates)
+                    int col = cw - OPS * m - O2 + k;
+                    col += col < 0 ? ny : 0;
+                    col -= col >= ny ? ny : 0;
                     for (int i = rlo + tr; i < rhi; i += RG) {
                         const int o = i * RS + k;
-                        Eq::step(cur + o - OPS, prv + o - O2, out + o, nb, gts, nv, a.p);
+                        if constexpr (Coords<Eq>::value) {
+                            int row = r0w + i;
+                            row -= row >= nx ? nx : 0;
+                            Eq::step_at(cur + o - OPS, prv + o - O2, out + o, nb, gts, nv, a.p, row,
+                                        col);
+                        } else {
+                            Eq::step(cur + o - OPS, prv + o - O2, out + o, nb, gts, nv, a.p);
+                        }
                     }
                 }
             }
@@ -607,7 +620,11 @@ __device__ __forceinline__ void seam_body(const SweptArgs& a, const int unit, T*
         }
         for_2d<NT>(nr, nc, tid, [&](int r, int c) {
             const int o = (rlo + r) * TW + clo + c;
-            Eq::step(cur + o, prv + o, out + o, nb, gts, nv, a.p);
+            if constexpr (Coords<Eq>::value)
+                Eq::step_at(cur + o, prv + o, out + o, nb, gts, nv, a.p, grow(rlo + r),
+                            gcol(clo + c));
+            else
+                Eq::step(cur + o, prv + o, out + o, nb, gts, nv, a.p);
         });
         if (!direct && m <= H - 1) {
             // y-faces of level m: left part from the left block's right edge,

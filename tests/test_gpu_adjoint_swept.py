@@ -1,0 +1,126 @@
+"""The swept form of the differentiable variable-diffusivity heat solve
+(adjoint.SweptHeatVar: the engine's heatvar and heatvar_adjoint equations
+through the prism / bridge / octahedron phases) against the standard fused
+kernels, bitwise, and against torch autograd."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _fields(n, seed):
+    import torch
+    rng = np.random.default_rng(seed)
+    x = np.arange(n) / n
+
+    def fourier(modes=8):
+        f = np.zeros((n, n))
+        for _ in range(modes):
+            k, l = rng.integers(1, 9, 2)
+            f += rng.uniform(0, 1) * np.sin(2 * np.pi * (k * x[:, None] + l * x[None, :]) +
+                                            rng.uniform(0, 2 * np.pi))
+        return f / modes
+    u0 = torch.tensor(fourier(), dtype=torch.float64, device="cuda")
+    alpha = torch.tensor(1.0 + 0.5 * fourier(), dtype=torch.float64, device="cuda")
+    target = torch.tensor(fourier(), dtype=torch.float64, device="cuda")
+    return u0, alpha, target
+
+
+def _grads(n, steps, every, swept, seed):
+    import torch
+    from pysweep_b200.adjoint import heat_solve
+    u0, alpha, target = _fields(n, seed)
+    dx = 1.0 / n
+    dt = 0.2 * dx * dx / 1.5
+    x = u0.clone().requires_grad_(True)
+    y = alpha.clone().requires_grad_(True)
+    uT = heat_solve(x, y, steps, dt, dx, every, swept=swept)
+    loss = 0.5 * ((uT - target) ** 2).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    return uT.detach(), x.grad, y.grad
+
+
+@pytest.mark.parametrize("n,steps,every", [(256, 100, 32), (256, 57, 16), (128, 40, 64),
+                                           (512, 30, 7)])
+def test_swept_solve_equals_standard_bitwise(n, steps, every):
+    a = _grads(n, steps, every, False, n + steps)
+    b = _grads(n, steps, every, True, n + steps)
+    for name, x, y in zip(("u_T", "dJ/du0", "dJ/dalpha"), a, b):
+        assert bool((x == y).all()), (name, (x - y).abs().max().item(), y.abs().max().item())
+
+
+def test_swept_gradients_match_torch_autograd():
+    import torch
+    from pysweep_b200.adjoint import heat_solve, heat_solve_reference
+    n, steps = 128, 60
+    u0, alpha, target = _fields(n, 5)
+    dx = 1.0 / n
+    dt = 0.2 * dx * dx / 1.5
+    g = []
+    for f in (lambda a, b: heat_solve(a, b, steps, dt, dx, 16, swept=True),
+              lambda a, b: heat_solve_reference(a, b, steps, dt, dx)):
+        x = u0.clone().requires_grad_(True)
+        y = alpha.clone().requires_grad_(True)
+        loss = 0.5 * ((f(x, y) - target) ** 2).sum()
+        loss.backward()
+        g.append((x.grad, y.grad))
+    for mine, ref in zip(g[0], g[1]):
+        rel = ((mine - ref).abs().max() / ref.abs().max()).item()
+        assert rel < 1e-11, rel
+
+
+def test_heatvar_engines_swept_equal_standard():
+    """The two equations through the engine: swept == standard, bitwise, for
+    every stored frame (heatvar) and for lambda and dJ/dC (the adjoint)."""
+    import torch
+    from pysweep_b200 import Engine
+    n, nl = 192, 29
+    u0, alpha, _ = _fields(n, 9)
+    C = (alpha * 1e-1).contiguous()
+    lap = {m: torch.zeros((nl, n, n), dtype=torch.float64, device="cuda") for m in ("swept", "standard")}
+    fr = {}
+    for mode in ("swept", "standard"):
+        e = Engine("heatvar", n, n, blocksize=32)
+        e.set_field(0, C)
+        e.set_field(1, lap[mode])
+        e.set_global("LEN", nl)
+        e.set_state(u0)
+        fr[mode] = np.zeros((nl, 1, n, n))
+        e.run(nl, mode=mode, frames=fr[mode])
+        e.close()
+    assert np.array_equal(fr["swept"], fr["standard"])
+    assert bool((lap["swept"] == lap["standard"]).all())
+    st = torch.stack([u0, torch.zeros_like(u0)]).contiguous()
+    out = {}
+    for mode in ("swept", "standard"):
+        a = Engine("heatvar_adjoint", n, n, blocksize=32)
+        a.set_field(0, C)
+        a.set_field(1, lap[mode])
+        a.set_global("LEN", nl)
+        a.set_state(st)
+        a.run(nl, mode=mode)
+        out[mode] = a.get_state()
+        a.close()
+    assert np.array_equal(out["swept"], out["standard"])
+    assert np.abs(out["swept"][1]).max() > 0
+
+
+def test_heatvar_needs_its_fields_and_levels():
+    import torch
+    from pysweep_b200 import Engine
+    from pysweep_b200._lib import PySweepError
+    e = Engine("heatvar_adjoint", 64, 64, blocksize=16)
+    e.set_state(np.zeros((2, 64, 64)))
+    with pytest.raises(PySweepError):
+        e.run(4)  # no fields
+    C = torch.full((64, 64), 0.1, dtype=torch.float64, device="cuda")
+    lap = torch.zeros((4, 64, 64), dtype=torch.float64, device="cuda")
+    e.set_field(0, C)
+    e.set_field(1, lap)
+    e.set_global("LEN", 4)
+    with pytest.raises(PySweepError):
+        e.run(5)  # more levels than the Laplacians hold
+    e.run(4)
+    e.synchronize()
+    e.close()
