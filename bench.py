@@ -891,13 +891,21 @@ def adjoint_line(args):
         sfwd.append(t_sf)
         sbwd.append(t_sb)
     t_sf, t_sb = statistics.median(sfwd), statistics.median(sbwd)
-    same = bool((su.grad == gu).all()) and bool((sa.grad == ga).all())
+    rel = lambda x, y: ((x - y).abs().max() / y.abs().max()).item()  # noqa: E731
+    # the lambda-form swept adjoint (generic kernels) once, untimed: bitwise
+    lu = u0.clone().requires_grad_(True)
+    la = alpha0.clone().requires_grad_(True)
+    (0.5 * ((heat_solve(lu, la, steps, dt, dx, every, swept="lambda") - target) ** 2).sum()).backward()
+    same = bool((lu.grad == gu).all()) and bool((la.grad == ga).all())
     return {
         "metric": "adjoint/forward cost", "value": t_b / t_f, "unit": "x", "higher_is_better": False,
         "forward_ms": t_f, "backward_ms": t_b, "n": n, "time_steps": steps, "checkpoint_every": every,
-        "swept": {"forward_ms": t_sf, "backward_ms": t_sb, "backward_over_swept_forward": t_sb / t_sf,
+        "swept": {"form": "mu", "forward_ms": t_sf, "backward_ms": t_sb,
+                  "backward_over_swept_forward": t_sb / t_sf,
                   "backward_over_fastest_forward": t_sb / min(t_f, t_sf),
-                  "gradients_equal_standard": same},
+                  "forward_equal_standard": bool((suT.detach() == uT.detach()).all()),
+                  "grad_u0_max_rel_diff": rel(su.grad, gu), "grad_alpha_max_rel_diff": rel(sa.grad, ga),
+                  "lambda_form_gradients_equal_standard": same},
         "fd_directions": args.adj_dirs, "fd_h": h, "fd_max_rel_err": worst,
         "fd_richardson_h": hr, "fd_richardson_max_rel_err": worst_r, "dtype": "f64",
         "data": "synthetic", "steps": args.steps, "warmup": args.warmup}

@@ -39,12 +39,14 @@ extern "C" {
 #define PS_EQ_EXAMPLE 2
 #define PS_EQ_CHECKER 3
 #define PS_EQ_HALF 4
-/* Heat with a courant number per cell (one variable) and its adjoint (two
- * variables: lambda and the accumulated dJ/dC), the kernels of the
- * differentiable solve (pysweep_b200.adjoint); their grid fields are set with
- * ps_set_field. */
+/* Heat with a courant number per cell (one variable) and its adjoint, the
+ * kernels of the differentiable solve (pysweep_b200.adjoint): in lambda (two
+ * variables: lambda and the accumulated dJ/dC) or in mu = C .* lambda (one
+ * variable; the sum of mu .* L(u) accumulates in grid field 2).  Their grid
+ * fields are set with ps_set_field. */
 #define PS_EQ_HEATVAR 6
 #define PS_EQ_HEATVAR_ADJ 7
+#define PS_EQ_HEATVAR_ADJMU 8
 
 /* Storage type of a solver's fields (ps_create_typed).  PS_DTYPE_F32 is the
  * reference's `dtype: float32` (pysweep/core/io.py:72-73): every level is
@@ -193,11 +195,13 @@ int ps_run(ps_solver *s, int mode, int64_t nlevels, int gts0, double *frames, in
  * numbers alpha*dt/dx^2 (both equations).  index 1: an array of
  * [LEN][nx][ny] (LEN: the solver's constant of that name, ps_set_global); for
  * PS_EQ_HEATVAR (NULL allowed) it receives, for every level gts a run
- * computes, the old level's Laplacian at index gts-1; PS_EQ_HEATVAR_ADJ (a
- * checkpoint segment of LEN steps, walked backward) reads the Laplacian of
- * level gts at index LEN-gts.  ps_run refuses runs whose levels
- * gts0 .. gts0+nlevels-1 fall outside 1 .. LEN.  No C-ABI counterpart in the
- * reference (its solver has no adjoint).
+ * computes, the old level's Laplacian at index gts-1; PS_EQ_HEATVAR_ADJ and
+ * PS_EQ_HEATVAR_ADJMU (a checkpoint segment of LEN steps, walked backward)
+ * read the Laplacian of level gts at index LEN-gts.  index 2
+ * (PS_EQ_HEATVAR_ADJMU): the [nx][ny] sum of mu_{n+1} .* L(u_n), updated in
+ * place.  ps_run refuses runs whose levels gts0 .. gts0+nlevels-1 fall
+ * outside 1 .. LEN.  No C-ABI counterpart in the reference (its solver has no
+ * adjoint).
  */
 int ps_set_field(ps_solver *s, int index, double *d_field);
 

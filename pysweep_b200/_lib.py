@@ -20,7 +20,7 @@ ERRORS = {
     -7: "call out of order",
 }
 EQ = {"heat": 0, "euler": 1, "example": 2, "checker": 3, "half": 4, "heatvar": 6,
-      "heatvar_adjoint": 7}
+      "heatvar_adjoint": 7, "heatvar_adjoint_mu": 8}
 MODE = {"swept": 0, "standard": 1}
 
 

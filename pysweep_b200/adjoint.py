@@ -30,34 +30,55 @@ def _call(fn, *args):
 
 class SweptHeatVar:
     """The same solve through the swept decomposition (the engine's prism,
-    bridge and octahedron phases; Engine equations "heatvar" and
-    "heatvar_adjoint", csrc/equations.cuh HeatVar / HeatVarAdj):
+    bridge and octahedron phases; Engine equations "heatvar",
+    "heatvar_adjoint_mu" and "heatvar_adjoint", csrc/equations.cuh):
 
-    * forward: u0 -> u_T with the courant field read by cell coordinates, the
-      state copied out every `every` steps (the checkpoints);
+    * forward: u0 -> u_T with a courant number per cell, the state copied out
+      every `every` steps (the checkpoints);
     * backward: for the segments from the last to the first, the segment's
       levels are recomputed from its checkpoint by the swept forward kernels,
-      which also store each old level's Laplacian L(u_n); then the adjoint
-      engine (state: lambda and dJ/dC) runs the segment backward through the
-      same decomposition, lambda_n = lambda_{n+1} + L(C lambda_{n+1}),
-      dJ/dC += lambda_{n+1} L(u_n).
+      which also store each old level's Laplacian L(u_n); then an adjoint
+      engine runs the segment backward through the same decomposition.
 
-    Every cell sees the standard kernels' operations in the same order, so
-    u_T, lambda_0 and dJ/dalpha equal those of the standard solve bitwise.
-    The work runs on a stream of its own, ordered after the caller's current
+    form="mu" (default): the adjoint in mu = C .* lambda,
+    mu_n = mu_{n+1} + C .* L(mu_{n+1}), the forward step itself, so it runs in
+    the forward's register-resident streams; the sum of mu_{n+1} .* L(u_n)
+    accumulates in place, and lambda_0 = mu_0 ./ C, dJ/dC = sum ./ C at the
+    end.  Same gradients as the standard kernels up to rounding (the products
+    C .* lambda are formed in another place).
+    form="lambda": lambda_n = lambda_{n+1} + L(C .* lambda_{n+1}),
+    dJ/dC += lambda_{n+1} .* L(u_n) in the generic swept kernels; every cell
+    sees the standard kernels' operations in the same order, so lambda_0 and
+    dJ/dalpha equal theirs bitwise.
+
+    The forward pass equals the standard forward bitwise in both forms.  The
+    work runs on a stream of its own, ordered after the caller's current
     stream on entry and before it on return."""
 
-    def __init__(self, nx, ny, every, blocksize=32, device=0):
+    def __init__(self, nx, ny, every, blocksize=32, device=0, form="mu"):
         from .engine import Engine
-        self.nx, self.ny, self.every, self.device = nx, ny, every, device
+        if form not in ("mu", "lambda"):
+            raise ValueError(f"form {form!r}: 'mu' or 'lambda'")
+        self.nx, self.ny, self.every, self.device, self.form = nx, ny, every, device, form
         # one stream for both engines (the recompute's Laplacians are read by
         # the adjoint engine's next run), ordered after the caller's stream
         self.stream = torch.cuda.Stream(device=device)
         self.fwd = Engine("heatvar", nx, ny, blocksize=blocksize, device=device)
-        self.adj = Engine("heatvar_adjoint", nx, ny, blocksize=blocksize, device=device)
+        self.adj = Engine("heatvar_adjoint_mu" if form == "mu" else "heatvar_adjoint", nx, ny,
+                          blocksize=blocksize, device=device)
         for e in (self.fwd, self.adj):
             e.set_stream(self.stream.cuda_stream)
         self.lap = None
+
+    @staticmethod
+    def levels_per_half_cycle(nx, ny, form="mu", device=0, blocksize=32):
+        """The swept engines' levels per half-cycle (both engines use the
+        same)."""
+        from .engine import Engine
+        e = Engine("heatvar", nx, ny, blocksize=blocksize, device=device)
+        h = e.tiling()["h"]
+        e.close()
+        return h
 
     def _enter(self):
         caller = torch.cuda.current_stream(self.device)
@@ -94,6 +115,7 @@ class SweptHeatVar:
     def backward(self, courant, ck, nsteps, lam_T):
         """(lambda_0, dJ/dC)."""
         nx, ny, every = self.nx, self.ny, self.every
+        mu = self.form == "mu"
         caller = self._enter()
         with torch.cuda.stream(self.stream):
             if self.lap is None:
@@ -104,8 +126,13 @@ class SweptHeatVar:
             f.set_global("LEN", every)
             a.set_field(0, courant)
             a.set_field(1, self.lap)
-            state = torch.zeros((2, nx, ny), dtype=lam_T.dtype, device=lam_T.device)
-            state[0].copy_(lam_T)
+            if mu:
+                state = courant * lam_T                 # mu_T = C .* lambda_T
+                acc = torch.zeros_like(lam_T)           # sum of mu_{n+1} .* L(u_n)
+                a.set_field(2, acc)
+            else:
+                state = torch.zeros((2, nx, ny), dtype=lam_T.dtype, device=lam_T.device)
+                state[0].copy_(lam_T)
             nseg = max(1, -(-nsteps // every))
             for sidx in range(nseg - 1, -1, -1):
                 n0 = sidx * every
@@ -116,10 +143,14 @@ class SweptHeatVar:
                 f.run(length)          # u_{n0+1..} and L(u_{n0..n0+length-1})
                 a.set_global("LEN", length)
                 a.set_state(state)
-                a.run(length)          # lambda_{n0+length} -> lambda_{n0}
+                a.run(length)          # segment end -> n0
                 a.get_state(out=state)
             f.set_field(1, None)
-            lam0, gC = state[0].clone(), state[1].clone()
+            if mu:
+                a.set_field(2, None)
+                lam0, gC = state / courant, acc / courant
+            else:
+                lam0, gC = state[0].clone(), state[1].clone()
         return self._leave(caller, lam0, gC)
 
     def close(self):
@@ -133,15 +164,23 @@ class HeatVarSolve(torch.autograd.Function):
         u0 = u0.contiguous()
         alpha = alpha.contiguous()
         nx, ny = u0.shape
-        nseg = max(1, -(-nsteps // every))
-        ck = torch.empty((nseg, nx, ny), dtype=u0.dtype, device=u0.device)
         if swept:
             courant = torch.empty_like(u0)
             _call(_lib.lib().ps_heatvar_courant, _p(alpha), _p(courant), nx, ny, dt, dx)
-            sw = SweptHeatVar(nx, ny, every, device=u0.device.index or 0)
+            form = "lambda" if swept == "lambda" else "mu"
+            # checkpoint segments of whole half-cycles (the values do not
+            # depend on the spacing; partial half-cycles cost a launch set
+            # for few levels)
+            h = SweptHeatVar.levels_per_half_cycle(nx, ny, form, u0.device.index or 0)
+            every = max(h, every - every % h)
+            sw = SweptHeatVar(nx, ny, every, device=u0.device.index or 0, form=form)
+            ck = torch.empty((max(1, -(-nsteps // every)), nx, ny), dtype=u0.dtype,
+                             device=u0.device)
             uT = sw.forward(u0, courant, nsteps, ck)
             ctx.sw = sw
         else:
+            ck = torch.empty((max(1, -(-nsteps // every)), nx, ny), dtype=u0.dtype,
+                             device=u0.device)
             courant = torch.empty_like(u0)
             work = torch.empty_like(u0)
             uT = torch.empty_like(u0)
@@ -174,10 +213,14 @@ class HeatVarSolve(torch.autograd.Function):
 
 def heat_solve(u0, alpha, nsteps, dt, dx, every=64, swept=False):
     """swept=False: the fused standard kernels (two levels per launch);
-    swept=True: the swept decomposition (SweptHeatVar).  Both give the same
-    values bitwise."""
+    swept=True or "mu": the swept decomposition with the adjoint in
+    mu = C .* lambda (SweptHeatVar, register-resident streams); swept="lambda":
+    the swept decomposition with the adjoint in lambda, bitwise equal to the
+    standard kernels.  The forward values are bitwise equal in all three."""
+    if swept not in (False, True, "mu", "lambda"):
+        raise ValueError(f"swept={swept!r}: False, True, 'mu' or 'lambda'")
     return HeatVarSolve.apply(u0, alpha, int(nsteps), float(dt), float(dx), int(every),
-                              bool(swept))
+                              swept if isinstance(swept, str) else bool(swept))
 
 
 def heat_solve_reference(u0, alpha, nsteps, dt, dx):

@@ -32,7 +32,7 @@ struct EqParams {
     // grid fields read (and written) by equations that address cells by their
     // coordinates (variable diffusivity and its adjoint); fs = elements of one
     // level of f[1]
-    double* f[2];
+    double* f[3];
     long long fs;
 };
 
@@ -50,7 +50,8 @@ enum EqId {
     EQ_CHECKER = 3,
     EQ_HALF = 4,
     EQ_HEATVAR = 6,
-    EQ_HEATVAR_ADJ = 7
+    EQ_HEATVAR_ADJ = 7,
+    EQ_HEATVAR_ADJMU = 8
 };
 
 // Equations whose step needs the cell's grid coordinates (Eq::kCoords and
@@ -475,6 +476,37 @@ struct HeatVarAdj {
         o[0] = __dadd_rn(l, lm);
         const double lu = __ldg(p.f[1] + (size_t)(p.i[3] - gts) * p.fs + at);
         o[n.vs] = __fma_rn(l, lu, u[n.vs]);
+    }
+};
+
+// The adjoint of HeatVar in the variable mu = C .* lambda: with L symmetric,
+// lambda_n = lambda_{n+1} + L(C .* lambda_{n+1}) is
+//     mu_n = mu_{n+1} + C .* L(mu_{n+1}),
+// HeatVar's own step (same operation order) applied to mu, and
+// dJ/dC = sum_n lambda_{n+1} .* L(u_n) = (sum_n mu_{n+1} .* L(u_n)) ./ C.
+// One variable (mu); level gts (1-based in a checkpoint segment of i[3] steps)
+// reads L(u_n), n = segment end - gts, at f[1][(i[3]-gts)*fs + row*ny + col]
+// and adds mu_{n+1} * L(u_n) to f[2][row*ny + col] in place (one fused
+// multiply-add per cell and level, in level order in every decomposition).
+// The register-resident streams (heat_fast.cuh, per-cell courant) do the
+// same arithmetic.  i[1] = nx, i[2] = ny.
+struct HeatVarAdjMu {
+    static constexpr int OPS = 1;
+    static constexpr int ID = EQ_HEATVAR_ADJMU;
+    static constexpr bool kCoords = true;
+    __device__ static __forceinline__ void step_at(const double* __restrict__ u,
+                                                   const double* __restrict__, double* __restrict__ o,
+                                                   const Nbr& n, int gts, int, const EqParams& p,
+                                                   int row, int col)
+    {
+        const size_t at = (size_t)row * p.i[2] + col;
+        const double c = u[0];
+        const double C = __ldg(p.f[0] + at);
+        const double rx = __dadd_rn(__fma_rn(-2.0, c, u[n.x[3]]), u[n.x[1]]);
+        const double ry = __dadd_rn(__fma_rn(-2.0, c, u[n.y[3]]), u[n.y[1]]);
+        o[0] = __dadd_rn(__dadd_rn(__dmul_rn(C, rx), __dmul_rn(C, ry)), c);
+        const double lu = __ldg(p.f[1] + (size_t)(p.i[3] - gts) * p.fs + at);
+        p.f[2][at] = __fma_rn(c, lu, p.f[2][at]);
     }
 };
 

@@ -115,6 +115,10 @@ __device__ __forceinline__ double from_left(double v, double carry, int lane)
 }
 
 constexpr int kFastWarps = 4;   // warps (units) per CTA
+// CTAs per SM the register cap allows: three for heat (168 registers), two
+// for the per-cell courant variants, whose extra operands would spill at 168
+template <int VAR>
+constexpr int kFastCtasPerSm = VAR == 0 ? 3 : 2;
 constexpr int kFastChunk = 64;  // columns per chunk
 constexpr int kFaceDepth = 3;   // gap: levels of face rows in flight ahead of use
 constexpr int kFaceSlots = kFaceDepth + 1;
@@ -166,6 +170,84 @@ __device__ __forceinline__ void heat_pair(double L1u, double L1c, double L1d, do
 {
     n0 = to_level<T>(heat_fe(L1c, L1u, L1d, L0c, c0, cr));
     n1 = to_level<T>(heat_fe(c0, u0, d0, L1c, c1, cr));
+}
+
+// Per-cell courant numbers (heat with a variable diffusivity, VAR > 0): the
+// courant field, this level's slab of the recomputed Laplacians (VAR 1: stored
+// when set; VAR 2: read) and the adjoint's accumulated sum (VAR 2).
+struct VarFields {
+    const double* C;
+    double* lu;
+    double* g;
+};
+
+// The per-cell operands of one new row at this lane's two columns, loaded one
+// row (the gap: one row pair) before they are used, so that their latency
+// overlaps the previous row's arithmetic: courant numbers and, for VAR 2, the
+// recomputed Laplacians.  (VAR 2's sums are read at the start of the row that
+// updates them: prefetching them too spills registers.)
+struct VarPre {
+    double c0, c1, l0, l1;
+};
+
+template <int VAR>
+__device__ __forceinline__ VarPre var_load(const VarFields& vf, int row, int ny, int gm, int gm1)
+{
+    VarPre p{};
+    if constexpr (VAR != 0) {
+        const size_t o = (size_t)row * ny;
+        p.c0 = __ldg(vf.C + o + gm);
+        p.c1 = __ldg(vf.C + o + gm1);
+        if constexpr (VAR == 2) {
+            p.l0 = __ldg(vf.lu + o + gm);
+            p.l1 = __ldg(vf.lu + o + gm1);
+        }
+    }
+    return p;
+}
+
+// heat_pair with the courant number of each cell (p.c0, p.c1); VAR 1 also
+// stores each old level's Laplacian (dxx + dyy before the courant factor, the
+// order of HeatVar::step_at) at grid row `row`, VAR 2 adds the old centre
+// times the recomputed Laplacian to the sum (HeatVarAdjMu::step_at).  Stores
+// only where `valid` (the lane's cells belong to this stream).
+template <int VAR>
+__device__ __forceinline__ void heat_pair_var(double L1u, double L1c, double L1d, double L0c,
+                                              double u0, double c0, double d0, double c1,
+                                              const VarPre& p, const VarFields& vf, int row,
+                                              int ny, int gm, int gm1, bool valid, double& n0,
+                                              double& n1)
+{
+    const size_t o = (size_t)row * ny;
+    double g0 = 0.0, g1 = 0.0;
+    if constexpr (VAR == 2) {  // issued before the row's arithmetic
+        g0 = vf.g[o + gm];
+        g1 = vf.g[o + gm1];
+    }
+    const double rx0 = __dadd_rn(__fma_rn(-2.0, L1c, L1d), L1u);
+    const double ry0 = __dadd_rn(__fma_rn(-2.0, L1c, c0), L0c);
+    const double rx1 = __dadd_rn(__fma_rn(-2.0, c0, d0), u0);
+    const double ry1 = __dadd_rn(__fma_rn(-2.0, c0, c1), L1c);
+    n0 = __dadd_rn(__dadd_rn(__dmul_rn(p.c0, rx0), __dmul_rn(p.c0, ry0)), L1c);
+    n1 = __dadd_rn(__dadd_rn(__dmul_rn(p.c1, rx1), __dmul_rn(p.c1, ry1)), c0);
+    if constexpr (VAR == 1) {
+        if (vf.lu && valid) {
+            vf.lu[o + gm] = __dadd_rn(rx0, ry0);
+            vf.lu[o + gm1] = __dadd_rn(rx1, ry1);
+        }
+    } else if constexpr (VAR == 2) {
+        if (valid) {
+            vf.g[o + gm] = __fma_rn(L1c, p.l0, g0);
+            vf.g[o + gm1] = __fma_rn(c0, p.l1, g1);
+        }
+    }
+}
+
+// Grid row of new row index k of the gap (row0: the grid row of index 0).
+__device__ __forceinline__ int gap_grid_row(int row0, int k, int nx)
+{
+    const int r = row0 + k;
+    return r >= nx ? r - nx : r;
 }
 
 // Gap: start the copy of the four prism face rows of level m at this lane's
@@ -246,9 +328,12 @@ __device__ __forceinline__ void store_bottom(int count, const double (&a0)[BX],
 // lane 0); on exit those of old rows K-2 and K-3, which the next pair needs
 // (old rows below K-1 are not written by this pair), so a pair takes four
 // new shuffles.
-template <int K, int BX, class T>
+template <int K, int BX, class T, int VAR = 0>
 __device__ __forceinline__ void gap_pair(double (&a0)[BX], double (&a1)[BX], const double* cr0,
-                                         int lane, double cr, double& L1a, double& L1b)
+                                         int lane, double cr, double& L1a, double& L1b,
+                                         VarPre& pa, VarPre& pb, const VarFields& vf = VarFields{},
+                                         int row0 = 0, int nx = 0, int ny = 0, int gm = 0,
+                                         int gm1 = 0, bool valid = false)
 {
     if constexpr (K >= 3 && K < BX) {
         const double L1d = L1a, L1c = L1b;
@@ -256,14 +341,29 @@ __device__ __forceinline__ void gap_pair(double (&a0)[BX], double (&a1)[BX], con
         const double L1u = from_left(a1[K - 2], cu.y, lane);
         const double L0c = from_left(a0[K - 1], cr0[(K - 1) * 2], lane);
         double n0, n1;
-        heat_pair<T>(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], cr, n0, n1);
+        // VAR: this pair's operands (pa: row K, pb: row K-1) were loaded one
+        // pair ago; the next pair's (rows K-2, K-3) are loaded now
+        const VarPre ca = pa, cb = pb;
+        if constexpr (VAR != 0) {
+            pa = var_load<VAR>(vf, gap_grid_row(row0, K - 2, nx), ny, gm, gm1);
+            pb = var_load<VAR>(vf, gap_grid_row(row0, K - 3, nx), ny, gm, gm1);
+        }
+        if constexpr (VAR == 0)
+            heat_pair<T>(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], cr, n0, n1);
+        else
+            heat_pair_var<VAR>(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], ca, vf,
+                               gap_grid_row(row0, K, nx), ny, gm, gm1, valid, n0, n1);
         a0[K] = n0;
         a1[K] = n1;
         // row K-1: up K-3, centre K-2, down K-1
         const double L1uu = from_left(a1[K - 3], cr0[(K - 3) * 2 + 1], lane);
         const double L0cc = from_left(a0[K - 2], cu.x, lane);
-        heat_pair<T>(L1uu, L1u, L1c, L0cc, a0[K - 3], a0[K - 2], a0[K - 1], a1[K - 2], cr, n0,
-                     n1);
+        if constexpr (VAR == 0)
+            heat_pair<T>(L1uu, L1u, L1c, L0cc, a0[K - 3], a0[K - 2], a0[K - 1], a1[K - 2], cr, n0,
+                         n1);
+        else
+            heat_pair_var<VAR>(L1uu, L1u, L1c, L0cc, a0[K - 3], a0[K - 2], a0[K - 1], a1[K - 2],
+                               cb, vf, gap_grid_row(row0, K - 1, nx), ny, gm, gm1, valid, n0, n1);
         a0[K - 1] = n0;
         a1[K - 1] = n1;
         L1a = L1u;
@@ -273,11 +373,17 @@ __device__ __forceinline__ void gap_pair(double (&a0)[BX], double (&a1)[BX], con
 
 // Gap: the left neighbours of old rows K and K-1, which the level's first
 // pair takes on entry.
-template <int K, int BX>
+template <int K, int BX, int VAR = 0>
 __device__ __forceinline__ void gap_entry(const double (&a1)[BX], const double* cr0, int lane,
-                                          double& L1a, double& L1b)
+                                          double& L1a, double& L1b, VarPre& pa, VarPre& pb,
+                                          const VarFields& vf = VarFields{}, int row0 = 0,
+                                          int nx = 0, int ny = 0, int gm = 0, int gm1 = 0)
 {
     if constexpr (K >= 3 && K < BX) {
+        if constexpr (VAR != 0) {  // the first pair's operands
+            pa = var_load<VAR>(vf, gap_grid_row(row0, K, nx), ny, gm, gm1);
+            pb = var_load<VAR>(vf, gap_grid_row(row0, K - 1, nx), ny, gm, gm1);
+        }
         L1a = from_left(a1[K], cr0[K * 2 + 1], lane);
         L1b = from_left(a1[K - 1], cr0[(K - 1) * 2 + 1], lane);
     }
@@ -287,10 +393,11 @@ __device__ __forceinline__ void gap_entry(const double (&a1)[BX], const double* 
 // segment's y-faces; `carry` is the warp's own shared memory
 // (heat_fast_warp_doubles: two packed carry buffers, then the ring).
 // T: storage type of the fields and faces (double or float).
-template <int BX, bool GAP, class T = double>
+template <int BX, bool GAP, class T = double, int VAR = 0>
 __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom sg,
                                                const int unit, double* carry)
 {
+    static_assert(VAR == 0 || sizeof(T) == 8, "per-cell courant numbers on float64 fields");
     using P = typename Pair2<T>::type;
     constexpr int hx = BX / 2;
     const int lane = threadIdx.x & 31;
@@ -379,6 +486,17 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
             // left-seam mask: the first chunk's level m starts at column s0+m
             // (lane m); a 32-column last chunk ends at lane 15
             const bool valid = (!first || lane >= m) && lane < nact;
+            // per-cell courant numbers: this level's slab of the Laplacians
+            // (VAR 1 stores level gts-1, VAR 2 reads level LEN-gts) and the
+            // adjoint's sum
+            VarFields vf{};
+            if constexpr (VAR != 0) {
+                const long long gts = a.gts_base + a.L0 + m;
+                vf.C = a.p.f[0];
+                const long long lvl = VAR == 1 ? gts - 1 : a.p.i[3] - gts;
+                vf.lu = a.p.f[1] ? a.p.f[1] + lvl * a.p.fs : nullptr;
+                vf.g = a.p.f[2];
+            }
             int nrow;  // rows of level m held in the arrays
             if (!GAP) {
                 // ---- prism: level m rows [m, BX-m) at indices [0, BX-2m) ----
@@ -389,6 +507,10 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                 double2 cc = *reinterpret_cast<const double2*>(cr0 + 2);
                 double L1u = from_left(a1[0], cu.y, lane);
                 double L1c = from_left(a1[1], cc.y, lane);
+                // VAR: grid row of band row m (new index 0) and its operands
+                int row = r0w + m;
+                row -= row >= nx ? nx : 0;
+                VarPre pn = var_load<VAR>(vf, row, ny, gm, gm1);
 #pragma unroll
                 for (int i = 0; i < BX - 2; ++i) {
                     if (i >= count) break;
@@ -396,8 +518,20 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                     const double L1d = from_left(a1[i + 2], cd.y, lane);
                     const double L0c = from_left(a0[i + 1], cc.x, lane);
                     double n0, n1;
-                    heat_pair<T>(L1u, L1c, L1d, L0c, a0[i], a0[i + 1], a0[i + 2], a1[i + 1], cr,
-                                 n0, n1);
+                    if constexpr (VAR == 0) {
+                        heat_pair<T>(L1u, L1c, L1d, L0c, a0[i], a0[i + 1], a0[i + 2], a1[i + 1],
+                                     cr, n0, n1);
+                    } else {
+                        // this row's operands were loaded one row ago; the
+                        // next row's are loaded now (past the last row: a
+                        // harmless in-bounds load)
+                        const VarPre pc = pn;
+                        const int rown = row + 1 == nx ? 0 : row + 1;
+                        pn = var_load<VAR>(vf, rown, ny, gm, gm1);
+                        heat_pair_var<VAR>(L1u, L1c, L1d, L0c, a0[i], a0[i + 1], a0[i + 2],
+                                           a1[i + 1], pc, vf, row, ny, gm, gm1, valid, n0, n1);
+                        row = rown;
+                    }
                     a0[i] = n0;
                     a1[i] = n1;
                     L1u = L1c;
@@ -412,16 +546,22 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                 // k-2 (up), k-1 (centre), k (down).
                 const int K0 = 2 * m + 1;
                 nrow = 2 * m + 2;
+                // grid row of new index 0 (band row hx-m-2)
+                int grow0 = r0w + hx - m - 2;
+                grow0 += grow0 < 0 ? nx : 0;
+                grow0 -= grow0 >= nx ? nx : 0;
                 // rows K0 .. 2, entered at K0 = 2m+1 (a prologue takes the first
                 // pair's two carried neighbours) and falling through
                 double L1a = 0.0, L1b = 0.0;
+                VarPre pa{}, pb{};  // VAR: the current pair's operands
 #define PSB_GAP_ENTRY(K)                                                                   \
     case K:                                                                                \
-        gap_entry<K, BX>(a1, cr0, lane, L1a, L1b);                                         \
+        gap_entry<K, BX, VAR>(a1, cr0, lane, L1a, L1b, pa, pb, vf, grow0, nx, ny, gm, gm1);  \
         goto pair_##K;
 #define PSB_GAP_PAIR(K)                                                                    \
     pair_##K:                                                                              \
-    gap_pair<K, BX, T>(a0, a1, cr0, lane, cr, L1a, L1b);
+    gap_pair<K, BX, T, VAR>(a0, a1, cr0, lane, cr, L1a, L1b, pa, pb, vf, grow0, nx, ny, gm,  \
+                            gm1, valid);
                 switch (K0) {
                     PSB_GAP_ENTRY(31) PSB_GAP_ENTRY(29) PSB_GAP_ENTRY(27) PSB_GAP_ENTRY(25)
                     PSB_GAP_ENTRY(23) PSB_GAP_ENTRY(21) PSB_GAP_ENTRY(19) PSB_GAP_ENTRY(17)
@@ -498,6 +638,8 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                     if (fr && valid) st_pair<T>(fr + o, gm, gm1, a0[i], a1[i], even);
                 }
             }
+            // VAR 2: the next level updates this level's sums from other lanes
+            if constexpr (VAR == 2) __syncwarp();
             // y-faces at the segment's column edges (read by the seam kernels)
             if (m <= H - 1 && (first || last)) {
 #pragma unroll
@@ -520,15 +662,18 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
     }
 }
 
-template <int BX, bool GAP, class T = double>
-__global__ void __launch_bounds__(32 * kFastWarps, 3) heat_stream_fast(SweptArgs a)
+// VAR 0: heat (one courant number); VAR 1: a courant number per cell
+// (HeatVar), storing each old level's Laplacian when p.f[1] is set; VAR 2: the
+// adjoint in mu = C .* lambda (HeatVarAdjMu).
+template <int BX, bool GAP, class T = double, int VAR = 0>
+__global__ void __launch_bounds__(32 * kFastWarps, kFastCtasPerSm<VAR>) heat_stream_fast(SweptArgs a)
 {
     extern __shared__ double sm[];
     const int warp = threadIdx.x >> 5;
     const int unit = blockIdx.x * kFastWarps + warp;
     if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
-    heat_fast_body<BX, GAP, T>(a, seg_geom(a, unit), unit,
-                               sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
+    heat_fast_body<BX, GAP, T, VAR>(a, seg_geom(a, unit), unit,
+                                    sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
 }  // namespace psb

@@ -71,7 +71,7 @@ struct ps_solver {
     int H = 0, nseg = 1, chunk = 32, threads = 128;
     // heatvar / heatvar adjoint: courant numbers, the segment's recomputed
     // Laplacians (ps_set_field; device memory the caller owns)
-    double* field[2] = {nullptr, nullptr};
+    double* field[3] = {nullptr, nullptr, nullptr};
     bool nseg_auto = true;  // choose the segment count per run until configured
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -170,6 +170,7 @@ int eq_ops(int eq, int ops)
     case PS_EQ_HALF: return 1;
     case PS_EQ_HEATVAR: return 1;
     case PS_EQ_HEATVAR_ADJ: return 1;
+    case PS_EQ_HEATVAR_ADJMU: return 1;
     case PS_EQ_EULER: return 2;
     default: return ops;  // example / checker take the configured ops
     }
@@ -211,13 +212,14 @@ EqParams make_params_g(int eq, const std::map<std::string, double>& globals)
 EqParams make_params(const ps_solver* s)
 {
     EqParams p = make_params_g(s->eq, s->globals);
-    if (s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJ) {
+    if (s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJ || s->eq == PS_EQ_HEATVAR_ADJMU) {
         p.i[1] = s->nx;
         p.i[2] = s->ny;
         auto it = s->globals.find("LEN");
         p.i[3] = it == s->globals.end() ? 0 : (int)it->second;
         p.f[0] = s->field[0];
         p.f[1] = s->field[1];
+        p.f[2] = s->field[2];
         p.fs = (long long)s->nx * s->ny;
     }
     return p;
@@ -264,10 +266,10 @@ struct SweptSet {
     bool fast = false;
 };
 
-template <int BX, bool GAP, class T = double>
+template <int BX, bool GAP, class T = double, int VAR = 0>
 void launch_fast(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
 {
-    auto k = heat_stream_fast<BX, GAP, T>;
+    auto k = heat_stream_fast<BX, GAP, T, VAR>;
     allow_big_smem(k);
     const int units = a.nb * a.nseg;
     k<<<(units + kFastWarps - 1) / kFastWarps, 32 * kFastWarps, smem, st>>>(a);
@@ -311,6 +313,8 @@ bool pick_swept(int eq, int ops, int its, int chunk, SweptSet* out)
     PS_SET(PS_EQ_HEATVAR, 1, 1, 64, HeatVar)
     PS_SET(PS_EQ_HEATVAR_ADJ, 1, 1, 32, HeatVarAdj)
     PS_SET(PS_EQ_HEATVAR_ADJ, 1, 1, 64, HeatVarAdj)
+    PS_SET(PS_EQ_HEATVAR_ADJMU, 1, 1, 32, HeatVarAdjMu)
+    PS_SET(PS_EQ_HEATVAR_ADJMU, 1, 1, 64, HeatVarAdjMu)
 #undef PS_SET
     return false;
 }
@@ -325,6 +329,7 @@ StdLaunch pick_standard(int eq, int ops)
     case PS_EQ_CHECKER: return ops == 2 ? launch_standard<CheckerT<2>> : launch_standard<CheckerT<1>>;
     case PS_EQ_HEATVAR: return launch_standard<HeatVar>;
     case PS_EQ_HEATVAR_ADJ: return launch_standard<HeatVarAdj>;
+    case PS_EQ_HEATVAR_ADJMU: return launch_standard<HeatVarAdjMu>;
     default: return nullptr;
     }
 }
@@ -424,7 +429,10 @@ int ensure_swept_buffers(ps_solver* s)
 // do not depend on the choice.
 int default_levels(int eq, int its, int bs, int mpss)
 {
-    if (eq == PS_EQ_HEAT && its == 1 && bs == 32) return std::min(mpss, 12);
+    // heat with forward Euler and the per-cell-courant variants share the
+    // register streams, measured fastest at 12 levels for blocksize 32
+    if ((eq == PS_EQ_HEAT || eq == PS_EQ_HEATVAR || eq == PS_EQ_HEATVAR_ADJMU) && its == 1 && bs == 32)
+        return std::min(mpss, 12);
     return mpss;
 }
 
@@ -547,6 +555,18 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
             K.P = launch_fast<32, false>;
             K.G = launch_fast<32, true>;
         }
+    } else if ((s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJMU) && s->threads != 256 &&
+               (s->bs == 16 || s->bs == 32) && s->ny % 32 == 0) {
+        // per-cell courant numbers in the register streams (the seams: the
+        // generic kernels with the same equation's step_at)
+        K.fast = true;
+        if (s->eq == PS_EQ_HEATVAR) {
+            K.P = s->bs == 16 ? launch_fast<16, false, double, 1> : launch_fast<32, false, double, 1>;
+            K.G = s->bs == 16 ? launch_fast<16, true, double, 1> : launch_fast<32, true, double, 1>;
+        } else {
+            K.P = s->bs == 16 ? launch_fast<16, false, double, 2> : launch_fast<32, false, double, 2>;
+            K.G = s->bs == 16 ? launch_fast<16, true, double, 2> : launch_fast<32, true, double, 2>;
+        }
     }
     if (s->H < 1 || s->H > s->mpss) return fail(s, PS_ERR_INVALID, "levels per half-cycle %d not in [1, %d]", s->H, s->mpss);
     if (s->chunk < O2 * (s->H + 1))
@@ -563,10 +583,12 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
                     s->ny / s->nseg, O2 * (s->H + 1));
     if (s->nseg_auto) {
         if (K.fast) {
-            // one warp per (band, segment); 3 CTAs of 4 warps per SM fit
+            // one warp per (band, segment); 3 CTAs of 4 warps per SM fit (2 for
+            // the per-cell courant variants)
             int sms = 148;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-            const int slots = sms * 3 * kFastWarps;
+            const bool var = s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJMU;
+            const int slots = sms * (var ? kFastCtasPerSm<1> : kFastCtasPerSm<0>) * kFastWarps;
             const int nb = s->nx / s->bs;
             s->nseg = std::max(1, std::min(s->ny / kFastChunk, slots / nb));
             s->nseg = std::max(1, std::min(s->nseg, s->ny / 32));
@@ -780,7 +802,7 @@ const GlobalSpec kGlobals[] = {
     {"DT", 0x1f},    {"DX", 0x1f},      {"DY", 0x1f},   {"ALPHA", 1 << PS_EQ_HEAT},
     {"SCHEME", (1 << PS_EQ_HEAT) | (1 << PS_EQ_EXAMPLE) | (1 << PS_EQ_CHECKER)},
     {"GAMMA", 1 << PS_EQ_EULER}, {"GAM_M1", 1 << PS_EQ_EULER}, {"DTDX", 1 << PS_EQ_EULER},
-    {"DTDY", 1 << PS_EQ_EULER}, {"LEN", (1 << PS_EQ_HEATVAR) | (1 << PS_EQ_HEATVAR_ADJ)},
+    {"DTDY", 1 << PS_EQ_EULER}, {"LEN", (1 << PS_EQ_HEATVAR) | (1 << PS_EQ_HEATVAR_ADJ) | (1 << PS_EQ_HEATVAR_ADJMU)},
 };
 
 const GlobalSpec* find_global(const ps_solver* s, const char* name)
@@ -903,7 +925,7 @@ int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, i
 {
     if (!out) return PS_ERR_INVALID;
     *out = nullptr;
-    if (equation < PS_EQ_HEAT || equation > PS_EQ_HEATVAR_ADJ || equation == PS_EQ_HOOK)
+    if (equation < PS_EQ_HEAT || equation > PS_EQ_HEATVAR_ADJMU || equation == PS_EQ_HOOK)
         return PS_ERR_INVALID;
     if (dtype != PS_DTYPE_F64 && dtype != PS_DTYPE_F32) return PS_ERR_INVALID;
     ps_solver* s = new ps_solver();
@@ -921,10 +943,13 @@ int ps_create_typed(ps_solver** out, int device, int equation, int nv, int nx, i
     if (equation == PS_EQ_HEAT || equation == PS_EQ_HALF) {
         if (nv != 1) rc = fail(s, PS_ERR_INVALID, "heat/half have one variable, got nv=%d", nv);
     }
-    if ((equation == PS_EQ_HEATVAR && nv != 1) || (equation == PS_EQ_HEATVAR_ADJ && nv != 2) ||
-        ((equation == PS_EQ_HEATVAR || equation == PS_EQ_HEATVAR_ADJ) && its != 1))
-        rc = fail(s, PS_ERR_INVALID, "heatvar has nv=1, its=1; its adjoint nv=2, its=1 (got nv=%d its=%d)",
-                  nv, its);
+    if (((equation == PS_EQ_HEATVAR || equation == PS_EQ_HEATVAR_ADJMU) && nv != 1) ||
+        (equation == PS_EQ_HEATVAR_ADJ && nv != 2) ||
+        ((equation == PS_EQ_HEATVAR || equation == PS_EQ_HEATVAR_ADJ || equation == PS_EQ_HEATVAR_ADJMU) &&
+         its != 1))
+        rc = fail(s, PS_ERR_INVALID,
+                  "heatvar and its mu-form adjoint have nv=1, the lambda-form adjoint nv=2; its=1 "
+                  "(got nv=%d its=%d)", nv, its);
     if (equation == PS_EQ_EULER && (nv != 4 || its != 2))
         rc = fail(s, PS_ERR_INVALID, "euler needs nv=4 and its=2 (got nv=%d its=%d)", nv, its);
     if (ops != s->ops) rc = fail(s, PS_ERR_INVALID, "equation %d has ops=%d, got %d", equation, s->ops, ops);
@@ -1232,9 +1257,9 @@ int ps_set_state(ps_solver* s, const double* src, int levels, int src_on_device)
 int ps_set_field(ps_solver* s, int index, double* d_field)
 {
     if (!s) return PS_ERR_INVALID;
-    if (s->eq != PS_EQ_HEATVAR && s->eq != PS_EQ_HEATVAR_ADJ)
+    if (s->eq != PS_EQ_HEATVAR && s->eq != PS_EQ_HEATVAR_ADJ && s->eq != PS_EQ_HEATVAR_ADJMU)
         return fail(s, PS_ERR_INVALID, "equation %d reads no grid fields", s->eq);
-    if (index < 0 || index > 1) return fail(s, PS_ERR_INVALID, "field index %d not 0 or 1", index);
+    if (index < 0 || index > 2) return fail(s, PS_ERR_INVALID, "field index %d not 0, 1 or 2", index);
     s->field[index] = d_field;
     return PS_OK;
 }
@@ -1246,11 +1271,13 @@ int ps_run(ps_solver* s, int mode, int64_t nlevels, int gts0, double* frames, in
     if (!s->have_state) return fail(s, PS_ERR_STATE, "ps_run before ps_set_state");
     if (nlevels < 0) return fail(s, PS_ERR_INVALID, "negative level count");
     if (frame_every < 0) return fail(s, PS_ERR_INVALID, "negative frame_every");
-    if ((s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJ) && !s->field[0])
-        return fail(s, PS_ERR_STATE, "heatvar: no courant field (ps_set_field 0)");
-    if (s->eq == PS_EQ_HEATVAR_ADJ && !s->field[1])
+    const bool hv = s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJ || s->eq == PS_EQ_HEATVAR_ADJMU;
+    if (hv && !s->field[0]) return fail(s, PS_ERR_STATE, "heatvar: no courant field (ps_set_field 0)");
+    if ((s->eq == PS_EQ_HEATVAR_ADJ || s->eq == PS_EQ_HEATVAR_ADJMU) && !s->field[1])
         return fail(s, PS_ERR_STATE, "heatvar adjoint: no recomputed Laplacians (ps_set_field 1)");
-    if ((s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJ) && s->field[1] && nlevels > 0) {
+    if (s->eq == PS_EQ_HEATVAR_ADJMU && !s->field[2])
+        return fail(s, PS_ERR_STATE, "heatvar adjoint (mu): no sum field (ps_set_field 2)");
+    if (hv && s->field[1] && nlevels > 0) {
         // field 1 holds LEN levels: the run's levels gts0 .. gts0+nlevels-1 must index them
         auto it = s->globals.find("LEN");
         const int64_t len = it == s->globals.end() ? 0 : (int64_t)it->second;

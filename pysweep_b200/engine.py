@@ -13,8 +13,10 @@ import numpy as np
 from . import _lib
 from ._lib import EQ, MODE, check
 
-DEFAULT_OPS = {"heat": 1, "half": 1, "euler": 2, "heatvar": 1, "heatvar_adjoint": 1}
-DEFAULT_NV = {"heat": 1, "half": 1, "euler": 4, "heatvar": 1, "heatvar_adjoint": 2}
+DEFAULT_OPS = {"heat": 1, "half": 1, "euler": 2, "heatvar": 1, "heatvar_adjoint": 1,
+               "heatvar_adjoint_mu": 1}
+DEFAULT_NV = {"heat": 1, "half": 1, "euler": 4, "heatvar": 1, "heatvar_adjoint": 2,
+              "heatvar_adjoint_mu": 1}
 
 
 def _is_torch_cuda(x):
@@ -90,9 +92,10 @@ class Engine:
         check(_lib.lib().ps_set_global(self._h, name.encode(), ctypes.byref(buf), n), self._h)
 
     def set_field(self, index, tensor):
-        """Grid field `index` of a heatvar / heatvar_adjoint engine (a device
-        tensor kept alive by the caller while runs are queued; None clears
-        it): 0 = courant numbers, 1 = the recomputed Laplacians (ps_set_field)."""
+        """Grid field `index` of a heatvar / heatvar_adjoint(_mu) engine (a
+        device tensor kept alive by the caller while runs are queued; None
+        clears it): 0 = courant numbers, 1 = the recomputed Laplacians, 2 = the
+        mu-form adjoint's sum (ps_set_field)."""
         ptr = None if tensor is None else ctypes.c_void_p(tensor.data_ptr())
         check(_lib.lib().ps_set_field(self._h, index, ptr), self._h)
 

@@ -1,7 +1,9 @@
 """The swept form of the differentiable variable-diffusivity heat solve
-(adjoint.SweptHeatVar: the engine's heatvar and heatvar_adjoint equations
-through the prism / bridge / octahedron phases) against the standard fused
-kernels, bitwise, and against torch autograd."""
+(adjoint.SweptHeatVar: the engine's heatvar, heatvar_adjoint_mu and
+heatvar_adjoint equations through the prism / bridge / octahedron phases)
+against the standard fused kernels (bitwise for the forward pass and the
+lambda-form adjoint, to 1e-12 for the mu-form adjoint, which forms C * lambda
+elsewhere) and against torch autograd."""
 import numpy as np
 import pytest
 
@@ -41,13 +43,25 @@ def _grads(n, steps, every, swept, seed):
     return uT.detach(), x.grad, y.grad
 
 
-@pytest.mark.parametrize("n,steps,every", [(256, 100, 32), (256, 57, 16), (128, 40, 64),
-                                           (512, 30, 7)])
-def test_swept_solve_equals_standard_bitwise(n, steps, every):
+CASES = [(256, 100, 32), (256, 57, 16), (128, 40, 64), (512, 30, 7)]
+
+
+@pytest.mark.parametrize("n,steps,every", CASES)
+def test_swept_lambda_form_equals_standard_bitwise(n, steps, every):
     a = _grads(n, steps, every, False, n + steps)
-    b = _grads(n, steps, every, True, n + steps)
+    b = _grads(n, steps, every, "lambda", n + steps)
     for name, x, y in zip(("u_T", "dJ/du0", "dJ/dalpha"), a, b):
         assert bool((x == y).all()), (name, (x - y).abs().max().item(), y.abs().max().item())
+
+
+@pytest.mark.parametrize("n,steps,every", CASES)
+def test_swept_mu_form_matches_standard(n, steps, every):
+    a = _grads(n, steps, every, False, n + steps)
+    b = _grads(n, steps, every, "mu", n + steps)
+    assert bool((a[0] == b[0]).all())  # the forward pass: bitwise
+    for name, x, y in zip(("dJ/du0", "dJ/dalpha"), a[1:], b[1:]):
+        rel = ((x - y).abs().max() / x.abs().max()).item()
+        assert rel < 1e-12, (name, rel)
 
 
 def test_swept_gradients_match_torch_autograd():
@@ -58,7 +72,7 @@ def test_swept_gradients_match_torch_autograd():
     dx = 1.0 / n
     dt = 0.2 * dx * dx / 1.5
     g = []
-    for f in (lambda a, b: heat_solve(a, b, steps, dt, dx, 16, swept=True),
+    for f in (lambda a, b: heat_solve(a, b, steps, dt, dx, 16, swept="mu"),
               lambda a, b: heat_solve_reference(a, b, steps, dt, dx)):
         x = u0.clone().requires_grad_(True)
         y = alpha.clone().requires_grad_(True)
@@ -104,6 +118,50 @@ def test_heatvar_engines_swept_equal_standard():
         a.close()
     assert np.array_equal(out["swept"], out["standard"])
     assert np.abs(out["swept"][1]).max() > 0
+
+
+@pytest.mark.parametrize("bs,n", [(32, 256), (16, 192)])
+def test_register_streams_per_cell_courant(bs, n):
+    """heatvar and heatvar_adjoint_mu in the register-resident streams against
+    the generic swept kernels (threads=256) and the standard path, bitwise:
+    the fields, every recomputed Laplacian and the adjoint's sum."""
+    import torch
+    from pysweep_b200 import Engine
+    nl = 40
+    u0, alpha, _ = _fields(n, 11 + bs)
+    C = (alpha * 1e-1).contiguous()
+    res = {}
+    for key, mode, threads in (("fast", "swept", 0), ("generic", "swept", 256),
+                               ("standard", "standard", 0)):
+        lap = torch.zeros((nl, n, n), dtype=torch.float64, device="cuda")
+        e = Engine("heatvar", n, n, blocksize=bs)
+        if threads:
+            e.configure(threads=threads)
+        e.set_field(0, C)
+        e.set_field(1, lap)
+        e.set_global("LEN", nl)
+        e.set_state(u0)
+        e.run(nl, mode=mode)
+        u = e.get_state()
+        e.close()
+        acc = torch.zeros_like(u0)
+        a = Engine("heatvar_adjoint_mu", n, n, blocksize=bs)
+        if threads:
+            a.configure(threads=threads)
+        a.set_field(0, C)
+        a.set_field(1, lap)
+        a.set_field(2, acc)
+        a.set_global("LEN", nl)
+        a.set_state(u0)
+        a.run(nl, mode=mode)
+        mu = a.get_state()
+        a.close()
+        torch.cuda.synchronize()
+        res[key] = (u, lap.cpu().numpy(), mu, acc.cpu().numpy())
+    for key in ("generic", "standard"):
+        for x, y in zip(res["fast"], res[key]):
+            assert np.array_equal(x, y), key
+    assert np.abs(res["fast"][3]).max() > 0
 
 
 def test_heatvar_needs_its_fields_and_levels():
