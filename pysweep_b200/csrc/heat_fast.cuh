@@ -187,7 +187,7 @@ struct VarFields {
 // recomputed Laplacians.  (VAR 2's sums are read at the start of the row that
 // updates them: prefetching them too spills registers.)
 struct VarPre {
-    double c0, c1, l0, l1;
+    double c0, c1, l0, l1, g0, g1;
 };
 
 template <int VAR>
@@ -201,6 +201,8 @@ __device__ __forceinline__ VarPre var_load(const VarFields& vf, int row, int ny,
         if constexpr (VAR == 2) {
             p.l0 = __ldg(vf.lu + o + gm);
             p.l1 = __ldg(vf.lu + o + gm1);
+            p.g0 = vf.g[o + gm];
+            p.g1 = vf.g[o + gm1];
         }
     }
     return p;
@@ -219,11 +221,7 @@ __device__ __forceinline__ void heat_pair_var(double L1u, double L1c, double L1d
                                               double& n1)
 {
     const size_t o = (size_t)row * ny;
-    double g0 = 0.0, g1 = 0.0;
-    if constexpr (VAR == 2) {  // issued before the row's arithmetic
-        g0 = vf.g[o + gm];
-        g1 = vf.g[o + gm1];
-    }
+    const double g0 = p.g0, g1 = p.g1;
     const double rx0 = __dadd_rn(__fma_rn(-2.0, L1c, L1d), L1u);
     const double ry0 = __dadd_rn(__fma_rn(-2.0, L1c, c0), L0c);
     const double rx1 = __dadd_rn(__fma_rn(-2.0, c0, d0), u0);
