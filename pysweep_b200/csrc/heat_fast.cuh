@@ -149,6 +149,28 @@ constexpr size_t heat_fast_smem(int hmax)
     return sizeof(double) * (size_t)kFastWarps * heat_fast_warp_doubles<BX>(hmax);
 }
 
+// Per-cell courant variants (VAR > 0): after the warp's carry buffers and face
+// ring, a ring of kVarSlots rows of per-cell operands ([field][lane]: the
+// courant numbers of the lane's two cells; for VAR 2 also the recomputed
+// Laplacians and the sums), copied by cp.async kVarAhead rows before use.
+constexpr int kVarSlots = 4;
+constexpr int kVarAhead = kVarSlots - 1;
+template <int VAR>
+__host__ __device__ constexpr int var_fields()
+{
+    return VAR == 2 ? 6 : (VAR == 1 ? 2 : 0);
+}
+template <int BX, int VAR>
+__host__ __device__ constexpr int heat_fast_warp_doubles_v(int hmax)
+{
+    return heat_fast_warp_doubles<BX>(hmax) + kVarSlots * var_fields<VAR>() * 32;
+}
+template <int BX, int VAR>
+constexpr size_t heat_fast_smem_v(int hmax)
+{
+    return sizeof(double) * (size_t)kFastWarps * heat_fast_warp_doubles_v<BX, VAR>(hmax);
+}
+
 // one pair of T (16 bytes for double, 8 for float)
 template <class T>
 __device__ __forceinline__ void cp_async_pair(T* smem, const T* gmem)
@@ -181,30 +203,58 @@ struct VarFields {
     double* g;
 };
 
-// The per-cell operands of one new row at this lane's two columns, loaded one
-// row (the gap: one row pair) before they are used, so that their latency
-// overlaps the previous row's arithmetic: courant numbers and, for VAR 2, the
-// recomputed Laplacians.  (VAR 2's sums are read at the start of the row that
-// updates them: prefetching them too spills registers.)
+// The per-cell operands of one new row at this lane's two columns.
 struct VarPre {
     double c0, c1, l0, l1, g0, g1;
 };
 
+// Start copying row `row`'s operands at the lane's columns gm, gm1 into one
+// ring slot (8-byte cp.async: the columns of odd levels are not 16-byte
+// aligned).  A sum is read here and written by this lane alone within the
+// level (other lanes' writes of the level before precede the level's first
+// copy, behind a __syncwarp).
 template <int VAR>
-__device__ __forceinline__ VarPre var_load(const VarFields& vf, int row, int ny, int gm, int gm1)
+__device__ __forceinline__ void var_issue(const VarFields& vf, double* slot, int row, int ny,
+                                          int gm, int gm1, int lane)
+{
+    const size_t o = (size_t)row * ny;
+    cp_async8(slot + 0 * 32 + lane, vf.C + o + gm);
+    cp_async8(slot + 1 * 32 + lane, vf.C + o + gm1);
+    if constexpr (VAR == 2) {
+        cp_async8(slot + 2 * 32 + lane, vf.lu + o + gm);
+        cp_async8(slot + 3 * 32 + lane, vf.lu + o + gm1);
+        cp_async8(slot + 4 * 32 + lane, vf.g + o + gm);
+        cp_async8(slot + 5 * 32 + lane, vf.g + o + gm1);
+    }
+}
+
+template <int VAR>
+__device__ __forceinline__ VarPre var_read(const double* slot, int lane)
 {
     VarPre p{};
-    if constexpr (VAR != 0) {
-        const size_t o = (size_t)row * ny;
-        p.c0 = __ldg(vf.C + o + gm);
-        p.c1 = __ldg(vf.C + o + gm1);
-        if constexpr (VAR == 2) {
-            p.l0 = __ldg(vf.lu + o + gm);
-            p.l1 = __ldg(vf.lu + o + gm1);
-            p.g0 = vf.g[o + gm];
-            p.g1 = vf.g[o + gm1];
-        }
+    p.c0 = slot[0 * 32 + lane];
+    p.c1 = slot[1 * 32 + lane];
+    if constexpr (VAR == 2) {
+        p.l0 = slot[2 * 32 + lane];
+        p.l1 = slot[3 * 32 + lane];
+        p.g0 = slot[4 * 32 + lane];
+        p.g1 = slot[5 * 32 + lane];
     }
+    return p;
+}
+
+// Ring position q of a level (the q-th row the level computes): wait until
+// its copy has landed, read it, and start the copy of position q + kVarAhead
+// (row `rnext`, if the level has it) into the slot read one position ago.
+template <int VAR>
+__device__ __forceinline__ VarPre var_next(const VarFields& vf, double* ring, int q, bool more,
+                                           int rnext, int ny, int gm, int gm1, int lane)
+{
+    constexpr int F = var_fields<VAR>() * 32;
+    cp_async_wait<kVarAhead - 1>();
+    const VarPre p = var_read<VAR>(ring + (q % kVarSlots) * F, lane);
+    if (more) var_issue<VAR>(vf, ring + ((q + kVarAhead) % kVarSlots) * F, rnext, ny, gm, gm1, lane);
+    cp_async_commit();
     return p;
 }
 
@@ -329,9 +379,9 @@ __device__ __forceinline__ void store_bottom(int count, const double (&a0)[BX],
 template <int K, int BX, class T, int VAR = 0>
 __device__ __forceinline__ void gap_pair(double (&a0)[BX], double (&a1)[BX], const double* cr0,
                                          int lane, double cr, double& L1a, double& L1b,
-                                         VarPre& pa, VarPre& pb, const VarFields& vf = VarFields{},
-                                         int row0 = 0, int nx = 0, int ny = 0, int gm = 0,
-                                         int gm1 = 0, bool valid = false)
+                                         const VarFields& vf = VarFields{}, double* vring = nullptr,
+                                         int K0 = 0, int row0 = 0, int nx = 0, int ny = 0,
+                                         int gm = 0, int gm1 = 0, bool valid = false)
 {
     if constexpr (K >= 3 && K < BX) {
         const double L1d = L1a, L1c = L1b;
@@ -339,29 +389,31 @@ __device__ __forceinline__ void gap_pair(double (&a0)[BX], double (&a1)[BX], con
         const double L1u = from_left(a1[K - 2], cu.y, lane);
         const double L0c = from_left(a0[K - 1], cr0[(K - 1) * 2], lane);
         double n0, n1;
-        // VAR: this pair's operands (pa: row K, pb: row K-1) were loaded one
-        // pair ago; the next pair's (rows K-2, K-3) are loaded now
-        const VarPre ca = pa, cb = pb;
-        if constexpr (VAR != 0) {
-            pa = var_load<VAR>(vf, gap_grid_row(row0, K - 2, nx), ny, gm, gm1);
-            pb = var_load<VAR>(vf, gap_grid_row(row0, K - 3, nx), ny, gm, gm1);
-        }
-        if constexpr (VAR == 0)
+        if constexpr (VAR == 0) {
             heat_pair<T>(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], cr, n0, n1);
-        else
-            heat_pair_var<VAR>(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], ca, vf,
+        } else {
+            // rows K, K-1 are ring positions K0-K, K0-K+1; the level's last
+            // row is new index 2
+            const VarPre p = var_next<VAR>(vf, vring, K0 - K, K - kVarAhead >= 2,
+                                           gap_grid_row(row0, K - kVarAhead, nx), ny, gm, gm1, lane);
+            heat_pair_var<VAR>(L1u, L1c, L1d, L0c, a0[K - 2], a0[K - 1], a0[K], a1[K - 1], p, vf,
                                gap_grid_row(row0, K, nx), ny, gm, gm1, valid, n0, n1);
+        }
         a0[K] = n0;
         a1[K] = n1;
         // row K-1: up K-3, centre K-2, down K-1
         const double L1uu = from_left(a1[K - 3], cr0[(K - 3) * 2 + 1], lane);
         const double L0cc = from_left(a0[K - 2], cu.x, lane);
-        if constexpr (VAR == 0)
+        if constexpr (VAR == 0) {
             heat_pair<T>(L1uu, L1u, L1c, L0cc, a0[K - 3], a0[K - 2], a0[K - 1], a1[K - 2], cr, n0,
                          n1);
-        else
+        } else {
+            const VarPre p = var_next<VAR>(vf, vring, K0 - K + 1, K - 1 - kVarAhead >= 2,
+                                           gap_grid_row(row0, K - 1 - kVarAhead, nx), ny, gm, gm1,
+                                           lane);
             heat_pair_var<VAR>(L1uu, L1u, L1c, L0cc, a0[K - 3], a0[K - 2], a0[K - 1], a1[K - 2],
-                               cb, vf, gap_grid_row(row0, K - 1, nx), ny, gm, gm1, valid, n0, n1);
+                               p, vf, gap_grid_row(row0, K - 1, nx), ny, gm, gm1, valid, n0, n1);
+        }
         a0[K - 1] = n0;
         a1[K - 1] = n1;
         L1a = L1u;
@@ -373,14 +425,20 @@ __device__ __forceinline__ void gap_pair(double (&a0)[BX], double (&a1)[BX], con
 // pair takes on entry.
 template <int K, int BX, int VAR = 0>
 __device__ __forceinline__ void gap_entry(const double (&a1)[BX], const double* cr0, int lane,
-                                          double& L1a, double& L1b, VarPre& pa, VarPre& pb,
-                                          const VarFields& vf = VarFields{}, int row0 = 0,
-                                          int nx = 0, int ny = 0, int gm = 0, int gm1 = 0)
+                                          double& L1a, double& L1b,
+                                          const VarFields& vf = VarFields{},
+                                          double* vring = nullptr, int row0 = 0, int nx = 0,
+                                          int ny = 0, int gm = 0, int gm1 = 0)
 {
     if constexpr (K >= 3 && K < BX) {
-        if constexpr (VAR != 0) {  // the first pair's operands
-            pa = var_load<VAR>(vf, gap_grid_row(row0, K, nx), ny, gm, gm1);
-            pb = var_load<VAR>(vf, gap_grid_row(row0, K - 1, nx), ny, gm, gm1);
+        if constexpr (VAR != 0) {  // ring positions 0 .. kVarAhead-1: rows K, K-1, ...
+            constexpr int F = var_fields<VAR>() * 32;
+#pragma unroll
+            for (int q = 0; q < kVarAhead; ++q) {
+                if (K - q >= 2) var_issue<VAR>(vf, vring + q * F, gap_grid_row(row0, K - q, nx), ny,
+                                               gm, gm1, lane);
+                cp_async_commit();
+            }
         }
         L1a = from_left(a1[K], cr0[K * 2 + 1], lane);
         L1b = from_left(a1[K - 1], cr0[(K - 1) * 2 + 1], lane);
@@ -414,6 +472,8 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                             ? carry_rows<BX, false>(Hm)
                             : carry_rows<BX, true>(Hm));
     T* ring = reinterpret_cast<T*>(carry + 2 * CB);  // gap: [kFaceSlots][4][32][2] of T
+    // VAR: the per-cell operand ring, after the warp's base share
+    double* vring = carry + heat_fast_warp_doubles<BX>(Hm);
     const int HF = Hm - 1;
     const int bup = wrap(band - 1, a.nb);
     const int r0w = wrap(r0, nx);
@@ -505,10 +565,20 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                 double2 cc = *reinterpret_cast<const double2*>(cr0 + 2);
                 double L1u = from_left(a1[0], cu.y, lane);
                 double L1c = from_left(a1[1], cc.y, lane);
-                // VAR: grid row of band row m (new index 0) and its operands
+                // VAR: grid row of band row m (new index 0); ring positions
+                // 0 .. kVarAhead-1 start arriving
                 int row = r0w + m;
                 row -= row >= nx ? nx : 0;
-                VarPre pn = var_load<VAR>(vf, row, ny, gm, gm1);
+                if constexpr (VAR != 0) {
+                    constexpr int F = var_fields<VAR>() * 32;
+#pragma unroll
+                    for (int q = 0; q < kVarAhead; ++q) {
+                        int rq = row + q;
+                        rq -= rq >= nx ? nx : 0;
+                        if (q < count) var_issue<VAR>(vf, vring + q * F, rq, ny, gm, gm1, lane);
+                        cp_async_commit();
+                    }
+                }
 #pragma unroll
                 for (int i = 0; i < BX - 2; ++i) {
                     if (i >= count) break;
@@ -520,15 +590,13 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                         heat_pair<T>(L1u, L1c, L1d, L0c, a0[i], a0[i + 1], a0[i + 2], a1[i + 1],
                                      cr, n0, n1);
                     } else {
-                        // this row's operands were loaded one row ago; the
-                        // next row's are loaded now (past the last row: a
-                        // harmless in-bounds load)
-                        const VarPre pc = pn;
-                        const int rown = row + 1 == nx ? 0 : row + 1;
-                        pn = var_load<VAR>(vf, rown, ny, gm, gm1);
+                        int ra = row + kVarAhead;  // grid row of ring position i + kVarAhead
+                        ra -= ra >= nx ? nx : 0;
+                        const VarPre pc = var_next<VAR>(vf, vring, i, i + kVarAhead < count, ra, ny,
+                                                        gm, gm1, lane);
                         heat_pair_var<VAR>(L1u, L1c, L1d, L0c, a0[i], a0[i + 1], a0[i + 2],
                                            a1[i + 1], pc, vf, row, ny, gm, gm1, valid, n0, n1);
-                        row = rown;
+                        row = row + 1 == nx ? 0 : row + 1;
                     }
                     a0[i] = n0;
                     a1[i] = n1;
@@ -551,15 +619,14 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                 // rows K0 .. 2, entered at K0 = 2m+1 (a prologue takes the first
                 // pair's two carried neighbours) and falling through
                 double L1a = 0.0, L1b = 0.0;
-                VarPre pa{}, pb{};  // VAR: the current pair's operands
 #define PSB_GAP_ENTRY(K)                                                                   \
     case K:                                                                                \
-        gap_entry<K, BX, VAR>(a1, cr0, lane, L1a, L1b, pa, pb, vf, grow0, nx, ny, gm, gm1);  \
+        gap_entry<K, BX, VAR>(a1, cr0, lane, L1a, L1b, vf, vring, grow0, nx, ny, gm, gm1);   \
         goto pair_##K;
 #define PSB_GAP_PAIR(K)                                                                    \
     pair_##K:                                                                              \
-    gap_pair<K, BX, T, VAR>(a0, a1, cr0, lane, cr, L1a, L1b, pa, pb, vf, grow0, nx, ny, gm,  \
-                            gm1, valid);
+    gap_pair<K, BX, T, VAR>(a0, a1, cr0, lane, cr, L1a, L1b, vf, vring, K0, grow0, nx, ny,   \
+                            gm, gm1, valid);
                 switch (K0) {
                     PSB_GAP_ENTRY(31) PSB_GAP_ENTRY(29) PSB_GAP_ENTRY(27) PSB_GAP_ENTRY(25)
                     PSB_GAP_ENTRY(23) PSB_GAP_ENTRY(21) PSB_GAP_ENTRY(19) PSB_GAP_ENTRY(17)
@@ -671,7 +738,7 @@ __global__ void __launch_bounds__(32 * kFastWarps, kFastCtasPerSm<VAR>) heat_str
     const int unit = blockIdx.x * kFastWarps + warp;
     if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
     heat_fast_body<BX, GAP, T, VAR>(a, seg_geom(a, unit), unit,
-                                    sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
+                                    sm + (size_t)warp * heat_fast_warp_doubles_v<BX, VAR>(a.Hmax));
 }
 
 }  // namespace psb

@@ -272,6 +272,8 @@ void launch_fast(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
     auto k = heat_stream_fast<BX, GAP, T, VAR>;
     allow_big_smem(k);
     const int units = a.nb * a.nseg;
+    // the per-cell courant variants add their operand ring to each warp's share
+    if (VAR) smem = heat_fast_smem_v<BX, VAR>(a.Hmax);
     k<<<(units + kFastWarps - 1) / kFastWarps, 32 * kFastWarps, smem, st>>>(a);
 }
 
