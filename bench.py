@@ -805,6 +805,56 @@ def run_adjoint(args):
     return 0
 
 
+def heatvar_line(args):
+    """The swept kernels of the differentiable solve alone: one segment of
+    `--adj-steps` levels at `--adj-n`^2 through Engine("heatvar") (the
+    recompute: courant numbers 0.1, every level's Laplacian stored) or
+    Engine("heatvar_adjoint_mu") (the adjoint: courant numbers, the
+    Laplacians and the sum set), from a seeded random field; one step = one
+    run of the segment.  Throughput and the per-kernel device time."""
+    import torch
+
+    from pysweep_b200 import Engine
+    n, nl = args.adj_n, args.adj_steps
+    rng = np.random.default_rng(0)
+    u0 = torch.tensor(rng.standard_normal((n, n)), device="cuda")
+    C = torch.full((n, n), 0.1, dtype=torch.float64, device="cuda")
+    lap = torch.zeros((nl, n, n), dtype=torch.float64, device="cuda")
+    acc = torch.zeros_like(u0)
+    eq = "heatvar" if args.heatvar == "fwd" else "heatvar_adjoint_mu"
+    e = Engine(eq, n, n, blocksize=32)
+    e.set_field(0, C)
+    e.set_field(1, lap)
+    e.set_global("LEN", nl)
+    if args.heatvar == "adj":
+        e.set_field(2, acc)
+    st = torch.cuda.Stream()
+    e.set_stream(st.cuda_stream)
+    for _ in range(args.warmup):
+        e.set_state(u0)
+        e.run(nl)
+    e.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(st)
+    for _ in range(args.steps):
+        e.set_state(u0)
+        e.run(nl)
+    ev1.record(st)
+    e.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    e.profile(True)
+    e.set_state(u0)
+    e.run(nl)
+    e.synchronize()
+    prof = {k: {"ms": v[0], "launches": v[1]} for k, v in e.profile_read().items() if v[1]}
+    tiling = e.tiling()
+    e.close()
+    return {"metric": f"{eq} swept Gcell-updates/s FP64", "value": n * n * nl / ms / 1e6,
+            "unit": "Gcell-updates/s", "ms_per_step": ms, "n": n, "levels": nl,
+            "tiling": tiling, "profile": prof, "dtype": "f64", "data": "synthetic",
+            "steps": args.steps, "warmup": args.warmup}
+
+
 def adjoint_line(args):
     """Inverse heat problem: forward vs adjoint cost, gradients vs central differences."""
     import torch
@@ -947,6 +997,9 @@ def main():
     ap.add_argument("--adj-n", type=int, default=2048)
     ap.add_argument("--adj-steps", type=int, default=2000)
     ap.add_argument("--adj-dirs", type=int, default=32)
+    ap.add_argument("--heatvar", choices=["fwd", "adj"], default=None,
+                    help="the differentiable solve's swept kernels alone: the recompute (fwd) or "
+                         "the adjoint (adj), one --adj-steps segment at --adj-n (separate JSON line)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
@@ -956,6 +1009,9 @@ def main():
         return run_batched(args)
     if args.adjoint:
         return run_adjoint(args)
+    if args.heatvar:
+        print(json.dumps(heatvar_line(args)), flush=True)
+        return 0
     if args.euler:
         return run_euler(args)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:
