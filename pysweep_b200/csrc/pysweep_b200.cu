@@ -15,6 +15,7 @@
 #include "equations.cuh"
 #include "swept.cuh"
 #include "heat_fast.cuh"
+#include "seam_fast.cuh"
 #include "standard_fast.cuh"
 #include "euler_faces.cuh"
 #include "batch.cuh"
@@ -275,6 +276,17 @@ void launch_fast(const SweptArgs& a, int grid, size_t smem, cudaStream_t st)
     // the per-cell courant variants add their operand ring to each warp's share
     if (VAR) smem = heat_fast_smem_v<BX, VAR>(a.Hmax);
     k<<<(units + kFastWarps - 1) / kFastWarps, 32 * kFastWarps, smem, st>>>(a);
+}
+
+// register-resident y-bridge seams of heat (seam_fast.cuh): one warp per
+// column edge, the staged y-faces in shared memory
+template <int BX>
+void launch_yseam(const SweptArgs& a, int grid, size_t, cudaStream_t st)
+{
+    auto k = heat_yseam_fast<BX>;
+    allow_big_smem(k);
+    const int units = a.nb * a.nseg;
+    k<<<(units + kSeamWarps - 1) / kSeamWarps, 32 * kSeamWarps, yseam_smem<BX>(a.Hmax), st>>>(a);
 }
 
 template <class Eq, int ITS, int W>
@@ -553,9 +565,11 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
         if (s->bs == 16) {
             K.P = launch_fast<16, false>;
             K.G = launch_fast<16, true>;
+            K.Y = launch_yseam<16>;
         } else {
             K.P = launch_fast<32, false>;
             K.G = launch_fast<32, true>;
+            K.Y = launch_yseam<32>;
         }
     } else if ((s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJMU) && s->threads != 256 &&
                (s->bs == 16 || s->bs == 32) && s->ny % 32 == 0) {
