@@ -289,6 +289,16 @@ void launch_yseam(const SweptArgs& a, int grid, size_t, cudaStream_t st)
     k<<<(units + kSeamWarps - 1) / kSeamWarps, 32 * kSeamWarps, yseam_smem<BX>(a.Hmax), st>>>(a);
 }
 
+// register-resident octahedron seams of heat (seam_fast.cuh)
+template <int BX>
+void launch_oseam(const SweptArgs& a, int grid, size_t, cudaStream_t st)
+{
+    auto k = heat_oseam_fast<BX>;
+    allow_big_smem(k);
+    const int units = a.nb * a.nseg;
+    k<<<(units + kSeamWarps - 1) / kSeamWarps, 32 * kSeamWarps, yseam_smem<BX>(a.Hmax), st>>>(a);
+}
+
 template <class Eq, int ITS, int W>
 SweptSet make_set()
 {
@@ -566,10 +576,12 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
             K.P = launch_fast<16, false>;
             K.G = launch_fast<16, true>;
             K.Y = launch_yseam<16>;
+            K.O = launch_oseam<16>;
         } else {
             K.P = launch_fast<32, false>;
             K.G = launch_fast<32, true>;
             K.Y = launch_yseam<32>;
+            K.O = launch_oseam<32>;
         }
     } else if ((s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJMU) && s->threads != 256 &&
                (s->bs == 16 || s->bs == 32) && s->ny % 32 == 0) {

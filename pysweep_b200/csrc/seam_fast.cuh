@@ -154,4 +154,190 @@ __global__ void __launch_bounds__(32 * kSeamWarps) heat_yseam_fast(SweptArgs a)
     heat_yseam_body<BX>(a, unit, sm + (size_t)warp * yseam_warp_doubles<BX>(a.Hmax));
 }
 
+// ---------------------------------------------------------------- octahedron
+// The Octahedron's down half (pysweep/core/pysweep.cu:164-217) at a column
+// edge of the gap band: level m computes rows [hx-m, hx+m) at columns
+// [KC-m, KC+m) (the shared-memory seam_kernel<Heat, 1, true>'s cells and
+// arithmetic).  Registers hold the gap stream's layout: before level m, index
+// k <-> row hx-m-1+k for k in [0, 2m+2) (indices 0, 1 and 2m, 2m+1: the
+// prisms' face rows of level m-1, x-faces); level m is computed in place from
+// index 2m+1 down to 2 (new index k <-> row hx-m-2+k reads old k-2, k-1, k),
+// entered at its first row through a switch.  After level m every lane of
+// columns [KC-m-2, KC+m+2) takes the four x-face rows of level m (loaded while
+// the level was computed) and the four lanes beside the level's columns take
+// the gap streams' y-faces of level m (staged in shared memory).
+
+// Lower face rows of level m at the dynamic indices 2m+2, 2m+3.
+#define PSB_OSEAM_LOWER(M)                                                                 \
+    case M:                                                                                \
+        if constexpr (2 * (M) + 3 < BX) {                                                  \
+            v[2 * (M) + 2] = f2;                                                           \
+            v[2 * (M) + 3] = f3;                                                           \
+        }                                                                                  \
+        break;
+
+template <int BX>
+__device__ __forceinline__ void oseam_lower(int m, double f2, double f3, double (&v)[BX])
+{
+    static_assert(BX <= 32, "cases cover blocksizes up to 32");
+    switch (m) {
+        PSB_OSEAM_LOWER(1) PSB_OSEAM_LOWER(2) PSB_OSEAM_LOWER(3) PSB_OSEAM_LOWER(4)
+        PSB_OSEAM_LOWER(5) PSB_OSEAM_LOWER(6) PSB_OSEAM_LOWER(7) PSB_OSEAM_LOWER(8)
+        PSB_OSEAM_LOWER(9) PSB_OSEAM_LOWER(10) PSB_OSEAM_LOWER(11) PSB_OSEAM_LOWER(12)
+        PSB_OSEAM_LOWER(13) PSB_OSEAM_LOWER(14)
+        default: break;
+    }
+}
+#undef PSB_OSEAM_LOWER
+
+template <int BX>
+__device__ __forceinline__ void heat_oseam_body(const SweptArgs& a, const int unit, double* ys)
+{
+    constexpr int hx = BX / 2;
+    const int lane = threadIdx.x & 31;
+    const int H = a.H, Hm = a.Hmax, nx = a.nx, ny = a.ny;
+    const int KC = Hm + 1;
+    const int HF = Hm - 1;
+    const SegGeom sg = seg_geom(a, unit);
+    const int band = sg.band;
+    const int bup = wrap(band - 1, a.nb);
+    const int r0w = wrap(a.off + band * BX - hx, nx);  // gap band row 0
+    const double cr = a.p.d[0];
+    const int gc = wrap(sg.s0 - KC + lane, ny);  // this lane's grid column
+    auto grow = [&](int r) {
+        int row = r0w + r;
+        row -= row >= nx ? nx : 0;
+        return row;
+    };
+    {
+        const double* yl = a.yface + ((size_t)sg.left * 2 + 1) * HF * BX * 2;
+        const double* yr = a.yface + ((size_t)unit * 2 + 0) * HF * BX * 2;
+        const int npair = (H - 1) * BX;
+        for (int e = lane; e < npair; e += 32) {
+            cp_async16(ys + e * 2, yl + e * 2);
+            cp_async16(ys + (HF * BX + e) * 2, yr + e * 2);
+        }
+        cp_async_commit();
+    }
+    // level 0: rows hx-2 .. hx+1 at columns KC-2 .. KC+1 (indices 0 .. 3)
+    double v[BX];
+#pragma unroll
+    for (int i = 0; i < BX; ++i) v[i] = 0.0;
+    if (lane >= KC - 2 && lane < KC + 2) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] = a.bin[(size_t)grow(hx - 2 + i) * ny + gc];
+    }
+    cp_async_wait<0>();
+    __syncwarp();
+    // x-face rows of level m at this lane's column: upper prism's bottom rows
+    // (j = 0, 1), lower prism's top rows
+    auto xrow = [&](int bb, int side, int j, int m) {
+        const size_t fo = (((size_t)bb * HF + (m - 1)) * 2 + side) * 2 + j;
+        return a.xface + fo * ny + xface_col(gc, m, ny);
+    };
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0, f3 = 0.0;
+    for (int m = 1; m <= H; ++m) {
+        // this level's x-faces, placed after the level (they are the next
+        // level's rows); loaded now so the level's arithmetic covers them
+        if (m <= H - 1) {
+            f0 = *xrow(bup, 1, 0, m);
+            f1 = *xrow(bup, 1, 1, m);
+            f2 = *xrow(band, 0, 0, m);
+            f3 = *xrow(band, 0, 1, m);
+        }
+        // ---- level m, in place from index 2m+1 down to 2 ---------------------
+#define PSB_OSEAM_ENTRY(M) \
+    case M:                \
+        goto orow_##M;
+#define PSB_OSEAM_ROW(K)                                                                   \
+    if constexpr ((K) >= 2 && (K) < BX) {                                                  \
+        const double c = v[(K) - 1];                                                       \
+        const double ym = __shfl_up_sync(0xffffffffu, c, 1);                               \
+        const double yp = __shfl_down_sync(0xffffffffu, c, 1);                             \
+        v[K] = heat_fe(c, v[(K) - 2], v[K], ym, yp, cr);                                   \
+    }
+        switch (m) {
+            PSB_OSEAM_ENTRY(15) PSB_OSEAM_ENTRY(14) PSB_OSEAM_ENTRY(13) PSB_OSEAM_ENTRY(12) PSB_OSEAM_ENTRY(11)
+            PSB_OSEAM_ENTRY(10) PSB_OSEAM_ENTRY(9) PSB_OSEAM_ENTRY(8) PSB_OSEAM_ENTRY(7)
+            PSB_OSEAM_ENTRY(6) PSB_OSEAM_ENTRY(5) PSB_OSEAM_ENTRY(4) PSB_OSEAM_ENTRY(3)
+            PSB_OSEAM_ENTRY(2) PSB_OSEAM_ENTRY(1)
+            default: goto orow_end;
+        }
+        // level m enters at index 2m+1 (label orow_m) and falls through to 2
+    orow_15:
+        PSB_OSEAM_ROW(31) PSB_OSEAM_ROW(30)
+    orow_14:
+        PSB_OSEAM_ROW(29) PSB_OSEAM_ROW(28)
+    orow_13:
+        PSB_OSEAM_ROW(27) PSB_OSEAM_ROW(26)
+    orow_12:
+        PSB_OSEAM_ROW(25) PSB_OSEAM_ROW(24)
+    orow_11:
+        PSB_OSEAM_ROW(23) PSB_OSEAM_ROW(22)
+    orow_10:
+        PSB_OSEAM_ROW(21) PSB_OSEAM_ROW(20)
+    orow_9:
+        PSB_OSEAM_ROW(19) PSB_OSEAM_ROW(18)
+    orow_8:
+        PSB_OSEAM_ROW(17) PSB_OSEAM_ROW(16)
+    orow_7:
+        PSB_OSEAM_ROW(15) PSB_OSEAM_ROW(14)
+    orow_6:
+        PSB_OSEAM_ROW(13) PSB_OSEAM_ROW(12)
+    orow_5:
+        PSB_OSEAM_ROW(11) PSB_OSEAM_ROW(10)
+    orow_4:
+        PSB_OSEAM_ROW(9) PSB_OSEAM_ROW(8)
+    orow_3:
+        PSB_OSEAM_ROW(7) PSB_OSEAM_ROW(6)
+    orow_2:
+        PSB_OSEAM_ROW(5) PSB_OSEAM_ROW(4)
+    orow_1:
+        PSB_OSEAM_ROW(3) PSB_OSEAM_ROW(2)
+    orow_end:;
+#undef PSB_OSEAM_ENTRY
+#undef PSB_OSEAM_ROW
+        const bool mine = lane >= KC - m && lane < KC + m;
+        // ---- base level of the next half-cycle and frames (indices [2, 2m+2):
+        // rows hx-m .. hx+m-1) ------------------------------------------------
+        const long long fs = frame_slot(a, a.L0 + m);
+        if ((m == H || fs >= 0) && mine) {
+            double* fr = fs >= 0 ? a.frames + (size_t)fs * nx * ny : nullptr;
+#pragma unroll
+            for (int k = 2; k < BX; ++k) {
+                if (k >= 2 * m + 2) break;
+                const size_t o = (size_t)grow(hx - m - 2 + k) * ny + gc;
+                if (m == H) a.bout[o] = v[k];
+                if (fr) fr[o] = v[k];
+            }
+        }
+        if (m <= H - 1) {
+            // the gap streams' y-faces of level m beside the level's columns
+            const int side = lane < KC ? 0 : 1;
+            const int j = side == 0 ? lane - (KC - m - 2) : lane - (KC + m);
+            const bool face = j >= 0 && j < 2;
+            const double* src = ys + ((side * HF + (m - 1)) * BX + hx - m) * 2 + (j & 1);
+#pragma unroll
+            for (int k = 2; k < BX; ++k) {
+                if (k >= 2 * m + 2) break;
+                if (face) v[k] = src[(k - 2) * 2];
+            }
+            // the prisms' face rows of level m: indices 0, 1 and 2m+2, 2m+3
+            v[0] = f0;
+            v[1] = f1;
+            oseam_lower<BX>(m, f2, f3, v);
+        }
+    }
+}
+
+template <int BX>
+__global__ void __launch_bounds__(32 * kSeamWarps) heat_oseam_fast(SweptArgs a)
+{
+    extern __shared__ double sm[];
+    const int warp = threadIdx.x >> 5;
+    const int unit = blockIdx.x * kSeamWarps + warp;
+    if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
+    heat_oseam_body<BX>(a, unit, sm + (size_t)warp * yseam_warp_doubles<BX>(a.Hmax));
+}
+
 }  // namespace psb
