@@ -10,6 +10,7 @@
 // layout.  The launches of a whole run are captured into one CUDA graph.
 #pragma once
 #include "heat_fast.cuh"
+#include "seam_fast.cuh"
 #include "swept.cuh"
 
 namespace psb {
@@ -40,6 +41,27 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3)
     batch_args<GAP>(desc, u.x, parity, H, L0, a);
     heat_fast_body<BX, GAP>(a, seg_geom(a, u.y), u.y,
                             sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
+}
+
+// The register-resident heat seams (seam_fast.cuh) over the unit table: one
+// warp per (instance, unit).  GAP selects the octahedron (role-1 descriptors).
+template <int BX, bool GAP>
+__global__ void __launch_bounds__(32 * kSeamWarps)
+    heat_seam_fast_batch(const SweptArgs* __restrict__ desc, const int2* __restrict__ units,
+                         int nunits, int parity, int H, long long L0)
+{
+    extern __shared__ double sm[];
+    const int warp = threadIdx.x >> 5;
+    const int g = blockIdx.x * kSeamWarps + warp;
+    if (g >= nunits) return;  // whole warp
+    const int2 u = units[g];
+    SweptArgs a;
+    batch_args<GAP>(desc, u.x, parity, H, L0, a);
+    double* ys = sm + (size_t)warp * yseam_warp_doubles<BX>(a.Hmax);
+    if constexpr (GAP)
+        heat_oseam_body<BX>(a, u.y, ys);
+    else
+        heat_yseam_body<BX>(a, u.y, ys);
 }
 
 // The generic batched kernels hold the descriptor fields in registers (the

@@ -1637,6 +1637,21 @@ void batch_half(ps_batch* b, int par, int H, long long L0, size_t ssm, size_t gs
         fork();
         stream_batch<Eq, ITS, W, true, 256><<<nu, 256, gsm, sd>>>(b->d_desc, b->d_units, par, H, L0);
     }
+    if (b->fast) {
+        // the register-resident seams, one warp per unit
+        const dim3 sgrid((nu + kSeamWarps - 1) / kSeamWarps);
+        const size_t ysm = b->bs == 16 ? yseam_smem<16>(b->H) : yseam_smem<32>(b->H);
+        if (b->bs == 16) {
+            heat_seam_fast_batch<16, false><<<sgrid, 32 * kSeamWarps, ysm, st>>>(b->d_desc, b->d_units, nu, par, H, L0);
+            join();
+            heat_seam_fast_batch<16, true><<<sgrid, 32 * kSeamWarps, ysm, st>>>(b->d_desc, b->d_units, nu, par, H, L0);
+        } else {
+            heat_seam_fast_batch<32, false><<<sgrid, 32 * kSeamWarps, ysm, st>>>(b->d_desc, b->d_units, nu, par, H, L0);
+            join();
+            heat_seam_fast_batch<32, true><<<sgrid, 32 * kSeamWarps, ysm, st>>>(b->d_desc, b->d_units, nu, par, H, L0);
+        }
+        return;
+    }
     seam_batch<Eq, ITS, false, 128><<<nu, 128, ssm, st>>>(b->d_desc, b->d_units, par, H, L0);
     join();
     seam_batch<Eq, ITS, true, 128><<<nu, 128, ssm, st>>>(b->d_desc, b->d_units, par, H, L0);
@@ -1649,6 +1664,10 @@ void batch_prepare()
     allow_big_smem(heat_stream_fast_batch<16, true>);
     allow_big_smem(heat_stream_fast_batch<32, false>);
     allow_big_smem(heat_stream_fast_batch<32, true>);
+    allow_big_smem(heat_seam_fast_batch<16, false>);
+    allow_big_smem(heat_seam_fast_batch<16, true>);
+    allow_big_smem(heat_seam_fast_batch<32, false>);
+    allow_big_smem(heat_seam_fast_batch<32, true>);
     allow_big_smem(stream_batch<Eq, ITS, W, false, 256>);
     allow_big_smem(stream_batch<Eq, ITS, W, true, 256>);
     allow_big_smem(seam_batch<Eq, ITS, false, 128>);
