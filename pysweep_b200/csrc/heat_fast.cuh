@@ -33,6 +33,11 @@
 // which hides the latency of the x-face reads.  The x-faces are stored at the
 // chunk's level-0 columns (xface_col in swept.cuh), so every face access is
 // one aligned 16-byte pair per lane.
+//
+// VAR 1 and 2 are the same streams with a courant number per cell (the
+// differentiable solve's forward step and its adjoint in mu = C .* lambda,
+// HeatVar and HeatVarAdjMu in equations.cuh): each row's per-cell operands
+// arrive through a ring in shared memory (var_issue / var_next).
 #pragma once
 #include "swept.cuh"
 
