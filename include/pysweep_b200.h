@@ -321,9 +321,19 @@ const char *ps_batch_last_error(const ps_batch *b);
  * ps_heatvar_courant: only the courant field, d_courant = d_alpha*dt/dx/dx
  * (the values ps_heatvar_forward writes), for the swept form of the same
  * solve (PS_EQ_HEATVAR / PS_EQ_HEATVAR_ADJ solvers).
+ *
+ * ps_heatvar_recompute: the recompute of one checkpoint segment for the
+ * swept adjoint: from d_u0 (the segment's checkpoint) runs `length` steps and
+ * stores the Laplacian of every old level k = 0 .. length-1 at
+ * d_lap[k][nx][ny] (the field 1 that PS_EQ_HEATVAR_ADJ(MU) solvers read);
+ * d_work holds two fields of scratch.  Two steps per launch, the fused
+ * forward kernels' arithmetic, so the Laplacians equal those the
+ * PS_EQ_HEATVAR solver stores.
  */
 int ps_heatvar_courant(const double *d_alpha, double *d_courant, int nx, int ny, double dt,
                        double dx, void *stream, char *err, size_t errlen);
+int ps_heatvar_recompute(const double *d_courant, const double *d_u0, double *d_lap, int length,
+                         int nx, int ny, double *d_work, void *stream, char *err, size_t errlen);
 int ps_heatvar_forward(const double *d_u0, const double *d_alpha, double *d_uT, int nx, int ny,
                        int64_t nsteps, double dt, double dx, double *d_courant, double *d_work,
                        double *d_checkpoints, int every, void *stream, char *err, size_t errlen);

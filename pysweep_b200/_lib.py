@@ -79,6 +79,10 @@ _SIGS = {
     "ps_heatvar_courant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "ps_heatvar_recompute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
+                                            ctypes.c_size_t]),
     "ps_heatvar_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int64,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_void_p,

@@ -36,9 +36,11 @@ class SweptHeatVar:
     * forward: u0 -> u_T with a courant number per cell, the state copied out
       every `every` steps (the checkpoints);
     * backward: for the segments from the last to the first, the segment's
-      levels are recomputed from its checkpoint by the swept forward kernels,
-      which also store each old level's Laplacian L(u_n); then an adjoint
-      engine runs the segment backward through the same decomposition.
+      levels are recomputed from its checkpoint, storing each old level's
+      Laplacian L(u_n) (ps_heatvar_recompute: the fused two-level forward
+      kernels, faster than the swept forward where the fields fit in L2, and
+      the same values); then an adjoint engine runs the segment backward
+      through the swept decomposition.
 
     form="mu" (default): the adjoint in mu = C .* lambda,
     mu_n = mu_{n+1} + C .* L(mu_{n+1}), the forward step itself, so it runs in
@@ -120,10 +122,8 @@ class SweptHeatVar:
         with torch.cuda.stream(self.stream):
             if self.lap is None:
                 self.lap = torch.empty((every, nx, ny), dtype=lam_T.dtype, device=lam_T.device)
-            f, a = self.fwd, self.adj
-            f.set_field(0, courant)
-            f.set_field(1, self.lap)
-            f.set_global("LEN", every)
+                self.work = torch.empty((2, nx, ny), dtype=lam_T.dtype, device=lam_T.device)
+            a = self.adj
             a.set_field(0, courant)
             a.set_field(1, self.lap)
             if mu:
@@ -139,13 +139,15 @@ class SweptHeatVar:
                 length = min(n0 + every, nsteps) - n0
                 if length <= 0:
                     continue
-                f.set_state(ck[sidx])
-                f.run(length)          # u_{n0+1..} and L(u_{n0..n0+length-1})
+                # L(u_{n0}) .. L(u_{n0+length-1}) from the checkpoint (the
+                # fused forward kernels: at sizes whose fields stay in L2 they
+                # outrun the swept forward, and the values are the same)
+                _call(_lib.lib().ps_heatvar_recompute, _p(courant), _p(ck[sidx]), _p(self.lap),
+                      length, nx, ny, _p(self.work))
                 a.set_global("LEN", length)
                 a.set_state(state)
                 a.run(length)          # segment end -> n0
                 a.get_state(out=state)
-            f.set_field(1, None)
             if mu:
                 a.set_field(2, None)
                 lam0, gC = state / courant, acc / courant

@@ -203,10 +203,13 @@ struct RowRing {
 };
 
 // u' = (C*dxx + C*dyy) + u.  Iteration x (rows x0 .. xend-1): u row x+1, C row x.
+// LAP: also store the old level's Laplacian (dxx + dyy before the courant
+// factor, the order of lap()) at lap_out.
+template <bool LAP = false>
 __global__ void __launch_bounds__(256) heatvar_step(const double* __restrict__ u,
                                                     const double* __restrict__ C,
                                                     double* __restrict__ out, int nx, int ny,
-                                                    int rows)
+                                                    int rows, double* __restrict__ lap_out = nullptr)
 {
     extern __shared__ double ring_sm[];
     const Strip s(nx, ny, rows);
@@ -235,6 +238,11 @@ __global__ void __launch_bounds__(256) heatvar_step(const double* __restrict__ u
         double n0, n1;
         fe_pair(up, ce, dn, cr.x, cr.y, s.lane, n0, n1);
         store_pair(out, s, s.x0 + t, n0, n1);
+        if (LAP) {
+            double l0, l1;
+            lap(up, ce, dn, s.lane, l0, l1);
+            store_pair(lap_out, s, s.x0 + t, l0, l1);
+        }
         up = ce;
         ce = dn;
     }
@@ -243,11 +251,15 @@ __global__ void __launch_bounds__(256) heatvar_step(const double* __restrict__ u
 // Two forward steps: mid = step(u), out = step(mid).  The first step runs on
 // rows x0-1 .. xend and on the halo columns.  Iteration i = x0-1+t: u row i+1
 // (two halo columns), C row i+1.
+// LAP: instead of the middle state, store the Laplacians of the two old
+// levels (u at lap_a, the middle state at lap_b).
+template <bool LAP = false>
 __global__ void __launch_bounds__(256) heatvar_step2(const double* __restrict__ u,
                                                      const double* __restrict__ C,
                                                      double* __restrict__ mid,
                                                      double* __restrict__ out, int nx, int ny,
-                                                     int rows)
+                                                     int rows, double* __restrict__ lap_a = nullptr,
+                                                     double* __restrict__ lap_b = nullptr)
 {
     extern __shared__ double ring_sm[];
     const Strip s(nx, ny, rows);
@@ -285,11 +297,24 @@ __global__ void __launch_bounds__(256) heatvar_step2(const double* __restrict__ 
         Row m;
         fe_pair(uu.row(), uc.row(), ud.row(), cc.a, cc.b, s.lane, m.a, m.b);
         m.h = fe_halo(uu, uc, ud, cc.h, s.lane);
-        if (i >= s.x0 && i < s.xend) store_pair(mid, s, i, m.a, m.b);
+        if (i >= s.x0 && i < s.xend) {
+            if (LAP) {
+                double l0, l1;
+                lap(uu.row(), uc.row(), ud.row(), s.lane, l0, l1);
+                store_pair(lap_a, s, i, l0, l1);
+            } else {
+                store_pair(mid, s, i, m.a, m.b);
+            }
+        }
         if (i > s.x0) {
             double o0, o1;
             fe_pair(mu, mc, m, cp.a, cp.b, s.lane, o0, o1);
             store_pair(out, s, i - 1, o0, o1);
+            if (LAP) {
+                double l0, l1;
+                lap(mu, mc, m, s.lane, l0, l1);
+                store_pair(lap_b, s, i - 1, l0, l1);
+            }
         }
         uu = uc;
         uc = ud;
@@ -536,6 +561,38 @@ extern "C" int ps_heatvar_courant(const double* d_alpha, double* d_courant, int 
     return adj_cuda(cudaGetLastError(), err, errlen);
 }
 
+extern "C" int ps_heatvar_recompute(const double* d_courant, const double* d_u0, double* d_lap,
+                                    int length, int nx, int ny, double* d_work, void* stream,
+                                    char* err, size_t errlen)
+{
+    int rc = adj_check(nx, ny, err, errlen);
+    if (rc) return rc;
+    if (!d_courant || !d_u0 || !d_lap || !d_work || length < 0) {
+        if (err && errlen) snprintf(err, errlen, "bad arguments");
+        return PS_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t n = (size_t)nx * ny;
+    const int rows = adj_rows(nx, ny, 8), rows_1 = adj_rows(nx, ny, 16);
+    const dim3 grid = strip_grid(nx, ny, rows), grid_1 = strip_grid(nx, ny, rows_1);
+    // two levels per launch (their Laplacians, then the state two levels on),
+    // the states ping-pong through the two work fields
+    const double* in = d_u0;
+    int w = 0, j = 0;
+    for (; j + 1 < length; j += 2) {
+        double* out = d_work + (size_t)w * n;
+        heatvar_step2<true><<<grid, 256, kStep2Smem, st>>>(in, d_courant, nullptr, out, nx, ny, rows,
+                                                          d_lap + (size_t)j * n,
+                                                          d_lap + (size_t)(j + 1) * n);
+        in = out;
+        w ^= 1;
+    }
+    if (j < length)
+        heatvar_step<true><<<grid_1, 256, kStepSmem, st>>>(in, d_courant, d_work + (size_t)w * n, nx,
+                                                          ny, rows_1, d_lap + (size_t)j * n);
+    return adj_cuda(cudaGetLastError(), err, errlen);
+}
+
 extern "C" int ps_heatvar_forward(const double* d_u0, const double* d_alpha, double* d_uT, int nx,
                                   int ny, int64_t nsteps, double dt, double dx, double* d_courant,
                                   double* d_work, double* d_checkpoints, int every, void* stream,
@@ -562,7 +619,7 @@ extern "C" int ps_heatvar_forward(const double* d_u0, const double* d_alpha, dou
                         err, errlen);
     for (int64_t k = 0; k < nsteps; ++k) {
         double* out = ((nsteps - 1 - k) % 2 == 0) ? d_uT : d_work;
-        heatvar_step<<<strip_grid(nx, ny, rows), 256, kStepSmem, st>>>(in, d_courant, out, nx, ny,
+        heatvar_step<false><<<strip_grid(nx, ny, rows), 256, kStepSmem, st>>>(in, d_courant, out, nx, ny,
                                                                        rows);
         if (d_checkpoints && (k + 1) % every == 0 && k + 1 < nsteps)
             if ((rc = adj_cuda(cudaMemcpyAsync(d_checkpoints + (size_t)((k + 1) / every) * n, out,
@@ -617,11 +674,11 @@ extern "C" int ps_heatvar_adjoint(const double* d_courant, const double* d_check
             return rc;
         int64_t j = 1;
         for (; j + 1 < len; j += 2)
-            heatvar_step2<<<grid, 256, kStep2Smem, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
+            heatvar_step2<false><<<grid, 256, kStep2Smem, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
                                                 d_states + (size_t)j * n,
                                                 d_states + (size_t)(j + 1) * n, nx, ny, rows);
         if (j < len)
-            heatvar_step<<<grid_1, 256, kStepSmem, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
+            heatvar_step<false><<<grid_1, 256, kStepSmem, st>>>(d_states + (size_t)(j - 1) * n, d_courant,
                                                          d_states + (size_t)j * n, nx, ny, rows_1);
         // adjoint levels k = len-1 .. 0 of the segment (lambda_{n0+k+1} -> lambda_{n0+k})
         int64_t k = len - 1;

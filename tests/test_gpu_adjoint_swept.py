@@ -182,3 +182,35 @@ def test_heatvar_needs_its_fields_and_levels():
     e.run(4)
     e.synchronize()
     e.close()
+
+
+@pytest.mark.parametrize("length", [1, 6, 13])
+def test_fused_recompute_laplacians_equal_swept_engine(length):
+    """ps_heatvar_recompute (the fused forward kernels) stores the same
+    Laplacians as the swept heatvar engine, bitwise."""
+    import ctypes
+
+    import torch
+    from pysweep_b200 import Engine, _lib
+    n = 256
+    u0, alpha, _ = _fields(n, 21 + length)
+    C = (alpha * 1e-1).contiguous()
+    lap_swept = torch.zeros((length, n, n), dtype=torch.float64, device="cuda")
+    e = Engine("heatvar", n, n, blocksize=32)
+    e.set_field(0, C)
+    e.set_field(1, lap_swept)
+    e.set_global("LEN", length)
+    e.set_state(u0)
+    e.run(length)
+    e.synchronize()
+    e.close()
+    lap_fused = torch.zeros_like(lap_swept)
+    work = torch.empty((2, n, n), dtype=torch.float64, device="cuda")
+    err = ctypes.create_string_buffer(256)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    rc = _lib.lib().ps_heatvar_recompute(p(C), p(u0), p(lap_fused), length, n, n, p(work),
+                                         ctypes.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                         err, 256)
+    assert rc == 0, err.value
+    torch.cuda.synchronize()
+    assert bool((lap_fused == lap_swept).all())
