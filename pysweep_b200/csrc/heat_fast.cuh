@@ -120,10 +120,15 @@ __device__ __forceinline__ double from_left(double v, double carry, int lane)
 }
 
 constexpr int kFastWarps = 4;   // warps (units) per CTA
-// CTAs per SM the register cap allows: three for heat (168 registers), two
-// for the per-cell courant variants, whose extra operands would spill at 168
-template <int VAR>
-constexpr int kFastCtasPerSm = VAR == 0 ? 3 : 2;
+// CTAs per SM the register cap allows.  Bands of 32 rows: three for heat (168
+// registers), two for the per-cell courant variants, whose extra operands
+// would spill at 168.  Bands of 16 rows hold half the values: four (128).
+__host__ __device__ constexpr int fast_ctas_per_sm(int bx, int var)
+{
+    return bx <= 16 ? 4 : (var == 0 ? 3 : 2);
+}
+template <int BX, int VAR>
+constexpr int kFastCtasPerSm = fast_ctas_per_sm(BX, VAR);
 constexpr int kFastChunk = 64;  // columns per chunk
 constexpr int kFaceDepth = 3;   // gap: levels of face rows in flight ahead of use
 constexpr int kFaceSlots = kFaceDepth + 1;
@@ -736,7 +741,7 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
 // (HeatVar), storing each old level's Laplacian when p.f[1] is set; VAR 2: the
 // adjoint in mu = C .* lambda (HeatVarAdjMu).
 template <int BX, bool GAP, class T = double, int VAR = 0>
-__global__ void __launch_bounds__(32 * kFastWarps, kFastCtasPerSm<VAR>) heat_stream_fast(SweptArgs a)
+__global__ void __launch_bounds__(32 * kFastWarps, kFastCtasPerSm<BX, VAR>) heat_stream_fast(SweptArgs a)
 {
     extern __shared__ double sm[];
     const int warp = threadIdx.x >> 5;

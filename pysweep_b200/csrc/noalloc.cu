@@ -77,7 +77,8 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int BX = blocksize, H = BX / 2 - 1, HF = H - 1, nb = nx / BX;
-    const int nseg = std::max(1, std::min(ny / kFastChunk, sms * 3 * kFastWarps / nb));
+    const int nseg =
+        std::max(1, std::min(ny / kFastChunk, sms * fast_ctas_per_sm(BX, 0) * kFastWarps / nb));
     const size_t field_b = round_up(fe * sizeof(double));
     const size_t xface_b = round_up((size_t)nb * HF * 2 * 2 * ny * sizeof(double));
     const size_t yface_b = round_up((size_t)nb * nseg * 2 * HF * BX * 2 * sizeof(double));

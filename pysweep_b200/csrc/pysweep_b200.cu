@@ -611,12 +611,12 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
                     s->ny / s->nseg, O2 * (s->H + 1));
     if (s->nseg_auto) {
         if (K.fast) {
-            // one warp per (band, segment); 3 CTAs of 4 warps per SM fit (2 for
-            // the per-cell courant variants)
+            // one warp per (band, segment); as many as the CTAs of 4 warps
+            // that fit on the SMs at once (fast_ctas_per_sm)
             int sms = 148;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
             const bool var = s->eq == PS_EQ_HEATVAR || s->eq == PS_EQ_HEATVAR_ADJMU;
-            const int slots = sms * (var ? kFastCtasPerSm<1> : kFastCtasPerSm<0>) * kFastWarps;
+            const int slots = sms * fast_ctas_per_sm(s->bs, var ? 1 : 0) * kFastWarps;
             const int nb = s->nx / s->bs;
             s->nseg = std::max(1, std::min(s->ny / kFastChunk, slots / nb));
             s->nseg = std::max(1, std::min(s->nseg, s->ny / 32));
