@@ -10,6 +10,7 @@ returns gradients with respect to u0 and alpha.  Tensors are FP64 CUDA
 tensors of shape (nx, ny), ny a multiple of 64.
 """
 import ctypes
+import functools
 
 import torch
 
@@ -76,11 +77,7 @@ class SweptHeatVar:
     def levels_per_half_cycle(nx, ny, form="mu", device=0, blocksize=32):
         """The swept engines' levels per half-cycle (both engines use the
         same)."""
-        from .engine import Engine
-        e = Engine("heatvar", nx, ny, blocksize=blocksize, device=device)
-        h = e.tiling()["h"]
-        e.close()
-        return h
+        return _levels_per_half_cycle(nx, ny, device, blocksize)
 
     def _enter(self):
         caller = torch.cuda.current_stream(self.device)
@@ -153,11 +150,49 @@ class SweptHeatVar:
                 lam0, gC = state / courant, acc / courant
             else:
                 lam0, gC = state[0].clone(), state[1].clone()
+            # the Laplacian slab (every fields) goes back to torch's cache of
+            # this stream; a cached solver does not hold it between solves
+            a.set_field(1, None)
+            self.lap = self.work = None
         return self._leave(caller, lam0, gC)
 
     def close(self):
         self.fwd.close()
         self.adj.close()
+
+
+@functools.lru_cache(maxsize=None)
+def _levels_per_half_cycle(nx, ny, device, blocksize):
+    from .engine import Engine
+    e = Engine("heatvar", nx, ny, blocksize=blocksize, device=device)
+    h = e.tiling()["h"]
+    e.close()
+    return h
+
+
+# Swept solvers of recent shapes, reused across solves: creating one
+# allocates its engines' device buffers (synchronising the device), which
+# costs as much as a short solve.  A solver evicted here lives on until no
+# pending backward pass holds it.
+_swept_cache = {}
+_SWEPT_CACHE_MAX = 4
+
+
+def _swept_solver(nx, ny, every, form, device):
+    key = (nx, ny, every, form, device)
+    sw = _swept_cache.pop(key, None)
+    if sw is None:
+        sw = SweptHeatVar(nx, ny, every, device=device, form=form)
+    _swept_cache[key] = sw  # most recently used last
+    while len(_swept_cache) > _SWEPT_CACHE_MAX:
+        _swept_cache.pop(next(iter(_swept_cache)))
+    return sw
+
+
+def release_swept_solvers():
+    """Drop the cached swept solvers; their device buffers are freed once no
+    pending backward pass holds them."""
+    _swept_cache.clear()
 
 
 class HeatVarSolve(torch.autograd.Function):
@@ -175,7 +210,7 @@ class HeatVarSolve(torch.autograd.Function):
             # for few levels)
             h = SweptHeatVar.levels_per_half_cycle(nx, ny, form, u0.device.index or 0)
             every = max(h, every - every % h)
-            sw = SweptHeatVar(nx, ny, every, device=u0.device.index or 0, form=form)
+            sw = _swept_solver(nx, ny, every, form, u0.device.index or 0)
             ck = torch.empty((max(1, -(-nsteps // every)), nx, ny), dtype=u0.dtype,
                              device=u0.device)
             uT = sw.forward(u0, courant, nsteps, ck)
@@ -200,7 +235,6 @@ class HeatVarSolve(torch.autograd.Function):
         g = grad_uT.contiguous()
         if ctx.sw is not None:
             lam0, gC = ctx.sw.backward(courant, ck, nsteps, g)
-            ctx.sw.close()
             ctx.sw = None
             # dJ/dalpha = dJ/dC * dt/dx/dx (scale_kernel's factor)
             return lam0, gC * (dt / dx / dx), None, None, None, None, None

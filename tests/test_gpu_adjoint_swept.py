@@ -214,3 +214,28 @@ def test_fused_recompute_laplacians_equal_swept_engine(length):
     assert rc == 0, err.value
     torch.cuda.synchronize()
     assert bool((lap_fused == lap_swept).all())
+
+
+def test_cached_swept_solver_serves_interleaved_solves():
+    """Two swept solves of one shape share a cached solver: both forward
+    passes first, then the backward passes in reverse order, give each solve
+    the gradients it gets alone."""
+    import torch
+    from pysweep_b200.adjoint import heat_solve, release_swept_solvers
+    n, steps, every = 256, 50, 24
+    dx = 1.0 / n
+    dt = 0.2 * dx * dx / 1.5
+    alone = [_grads(n, steps, every, "mu", seed) for seed in (3, 4)]
+    runs = []
+    for seed in (3, 4):
+        u0, alpha, target = _fields(n, seed)
+        x = u0.clone().requires_grad_(True)
+        y = alpha.clone().requires_grad_(True)
+        loss = 0.5 * ((heat_solve(x, y, steps, dt, dx, every, swept="mu") - target) ** 2).sum()
+        runs.append((loss, x, y))
+    for loss, _, _ in reversed(runs):
+        loss.backward()
+    torch.cuda.synchronize()
+    for (loss, x, y), (_, gx, gy) in zip(runs, alone):
+        assert bool((x.grad == gx).all()) and bool((y.grad == gy).all())
+    release_swept_solvers()
