@@ -326,33 +326,27 @@ __device__ __forceinline__ void issue_faces(const SweptArgs& a, int bup, int ban
     }
 }
 
-// Gap: the lower prism's two face rows of level m go to register indices
-// 2m+2 and 2m+3.  m is known only at run time, so a switch names each pair
-// with constant indices (register arrays cannot be indexed dynamically).
-#define PSB_LOWER_CASE(M)                                                                  \
-    case M:                                                                                \
-        if constexpr (2 * (M) + 3 < BX) {                                                  \
-            a0[2 * (M) + 2] = f2.x;                                                        \
-            a1[2 * (M) + 2] = f2.y;                                                        \
-            a0[2 * (M) + 3] = f3.x;                                                        \
-            a1[2 * (M) + 3] = f3.y;                                                        \
-        }                                                                                  \
-        break;
-
-template <int BX>
-__device__ __forceinline__ void place_lower(int m, double2 f2, double2 f3, double (&a0)[BX],
-                                            double (&a1)[BX])
+// Gap: the lower prism's two face rows of level m-1 join the arrays at
+// indices K-1 and K (K = 2m+1, the level's first pair), on the level's entry
+// path into the pairs: the write has constant register indices and sits on a
+// path of its own, so no other path has to merge it (a switch after the
+// level, joining all cases in one place, made the compiler select every
+// index it could write).  `lower` points at this lane's pair of the face
+// row in the ring slot of level m-1; at m = 1 the rows are the base rows
+// loaded with level 0.
+template <int K, int BX, class T>
+__device__ __forceinline__ void gap_lower(double (&a0)[BX], double (&a1)[BX], const T* lower)
 {
-    static_assert(BX <= 32, "cases cover blocksizes up to 32");
-    switch (m) {
-        PSB_LOWER_CASE(1) PSB_LOWER_CASE(2) PSB_LOWER_CASE(3) PSB_LOWER_CASE(4)
-        PSB_LOWER_CASE(5) PSB_LOWER_CASE(6) PSB_LOWER_CASE(7) PSB_LOWER_CASE(8)
-        PSB_LOWER_CASE(9) PSB_LOWER_CASE(10) PSB_LOWER_CASE(11) PSB_LOWER_CASE(12)
-        PSB_LOWER_CASE(13) PSB_LOWER_CASE(14)
-        default: break;
+    if constexpr (K >= 5 && K < BX) {
+        using P = typename Pair2<T>::type;
+        const double2 f2 = widen(*reinterpret_cast<const P*>(lower));
+        const double2 f3 = widen(*reinterpret_cast<const P*>(lower + 64));
+        a0[K - 1] = f2.x;
+        a1[K - 1] = f2.y;
+        a0[K] = f3.x;
+        a1[K] = f3.y;
     }
 }
-#undef PSB_LOWER_CASE
 
 // Prism: the bottom face rows of level m are the last two of its `count`
 // rows, register indices count-2 and count-1.
@@ -566,6 +560,7 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                 vf.g = a.p.f[2];
             }
             int nrow;  // rows of level m held in the arrays
+            double2 lower2 = make_double2(0.0, 0.0), lower3 = lower2;  // gap: lower face rows
             if (!GAP) {
                 // ---- prism: level m rows [m, BX-m) at indices [0, BX-2m) ----
                 // old index i <-> row m-1+i; new index i <-> row m+i
@@ -626,11 +621,14 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                 int grow0 = r0w + hx - m - 2;
                 grow0 += grow0 < 0 ? nx : 0;
                 grow0 -= grow0 >= nx ? nx : 0;
-                // rows K0 .. 2, entered at K0 = 2m+1 (a prologue takes the first
-                // pair's two carried neighbours) and falling through
+                // rows K0 .. 2, entered at K0 = 2m+1 (a prologue places the
+                // lower face rows of level m-1 and takes the first pair's two
+                // carried neighbours) and falling through
                 double L1a = 0.0, L1b = 0.0;
+                const T* lower = ring + ((m - 1) % kFaceSlots) * 256 + 2 * 64 + lane * 2;
 #define PSB_GAP_ENTRY(K)                                                                   \
     case K:                                                                                \
+        gap_lower<K, BX, T>(a0, a1, lower);                                                \
         gap_entry<K, BX, VAR>(a1, cr0, lane, L1a, L1b, vf, vring, grow0, nx, ny, gm, gm1);   \
         goto pair_##K;
 #define PSB_GAP_PAIR(K)                                                                    \
@@ -652,21 +650,22 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
             pairs_done:
 #undef PSB_GAP_ENTRY
 #undef PSB_GAP_PAIR
-                // the face rows of level m join: upper at indices 0, 1, lower at
-                // 2m+2, 2m+3 (the next level's first centre and down rows).
-                // Each lane reads back only the pairs it copied.
+                // the face rows of level m: the upper ones join at indices 0, 1;
+                // the lower ones (indices 2m+2, 2m+3, the next level's first
+                // centre and down rows) at the next level's entry, and in the
+                // carry from here.  Each lane reads back only the pairs it
+                // copied.
                 if (m <= H - 1) {
                     cp_async_wait<kFaceDepth - 1>();  // level m's group has landed
                     const T* sl = ring + (m % kFaceSlots) * 256 + lane * 2;
                     const double2 f0 = widen(*reinterpret_cast<const P*>(sl + 0 * 64));
                     const double2 f1 = widen(*reinterpret_cast<const P*>(sl + 1 * 64));
-                    const double2 f2 = widen(*reinterpret_cast<const P*>(sl + 2 * 64));
-                    const double2 f3 = widen(*reinterpret_cast<const P*>(sl + 3 * 64));
+                    lower2 = widen(*reinterpret_cast<const P*>(sl + 2 * 64));
+                    lower3 = widen(*reinterpret_cast<const P*>(sl + 3 * 64));
                     a0[0] = f0.x;
                     a1[0] = f0.y;
                     a0[1] = f1.x;
                     a1[1] = f1.y;
-                    place_lower<BX>(m, f2, f3, a0, a1);
                     // refill the slot of level m-1 (read one level ago)
                     const int mf = m + kFaceDepth;
                     if (mf <= H - 1)
@@ -676,12 +675,16 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
             }
             if (m <= H - 1 && !last) {
                 double* co = cout + carry_rows<BX, GAP>(m) * 2;
-                const int ncarry = GAP ? nrow + 2 : nrow;
 #pragma unroll
                 for (int i = 0; i < BX; ++i) {
-                    if (i >= ncarry) break;
+                    if (i >= nrow) break;
                     if (lane == 31)
                         *reinterpret_cast<double2*>(co + i * 2) = make_double2(a0[i], a1[i]);
+                }
+                // gap: the lower face rows complete the level's carry
+                if (GAP && lane == 31) {
+                    *reinterpret_cast<double2*>(co + nrow * 2) = lower2;
+                    *reinterpret_cast<double2*>(co + nrow * 2 + 2) = lower3;
                 }
             }
             // ---- outputs of level m ------------------------------------------

@@ -183,6 +183,8 @@ FAST = [
     (320, 16, 17, {"nseg": 4}),   # 5 chunks over 4 segments
     (384, 32, 40, {"nseg": 0}),   # automatic segment count
     (256, 32, 37, {"nseg": 1}),   # one segment: each seam joins a block to itself
+    (384, 16, 20, {"nseg": 0}),   # automatic segment count at four CTAs per SM
+    (1024, 16, 15, {}),           # 16 segments of one chunk per band
 ]
 
 
