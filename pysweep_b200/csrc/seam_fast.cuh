@@ -164,31 +164,10 @@ __global__ void __launch_bounds__(32 * kSeamWarps) heat_yseam_fast(SweptArgs a)
 // index 2m+1 down to 2 (new index k <-> row hx-m-2+k reads old k-2, k-1, k),
 // entered at its first row through a switch.  After level m every lane of
 // columns [KC-m-2, KC+m+2) takes the four x-face rows of level m (loaded while
-// the level was computed) and the four lanes beside the level's columns take
-// the gap streams' y-faces of level m (staged in shared memory).
-
-// Lower face rows of level m at the dynamic indices 2m+2, 2m+3.
-#define PSB_OSEAM_LOWER(M)                                                                 \
-    case M:                                                                                \
-        if constexpr (2 * (M) + 3 < BX) {                                                  \
-            v[2 * (M) + 2] = f2;                                                           \
-            v[2 * (M) + 3] = f3;                                                           \
-        }                                                                                  \
-        break;
-
-template <int BX>
-__device__ __forceinline__ void oseam_lower(int m, double f2, double f3, double (&v)[BX])
-{
-    static_assert(BX <= 32, "cases cover blocksizes up to 32");
-    switch (m) {
-        PSB_OSEAM_LOWER(1) PSB_OSEAM_LOWER(2) PSB_OSEAM_LOWER(3) PSB_OSEAM_LOWER(4)
-        PSB_OSEAM_LOWER(5) PSB_OSEAM_LOWER(6) PSB_OSEAM_LOWER(7) PSB_OSEAM_LOWER(8)
-        PSB_OSEAM_LOWER(9) PSB_OSEAM_LOWER(10) PSB_OSEAM_LOWER(11) PSB_OSEAM_LOWER(12)
-        PSB_OSEAM_LOWER(13) PSB_OSEAM_LOWER(14)
-        default: break;
-    }
-}
-#undef PSB_OSEAM_LOWER
+// the level was computed; the lower two join at the next level's entry, on
+// the path of the switch case that enters it, as in the gap stream) and the
+// four lanes beside the level's columns take the gap streams' y-faces of
+// level m (staged in shared memory).
 
 template <int BX>
 __device__ __forceinline__ void heat_oseam_body(const SweptArgs& a, const int unit, double* ys)
@@ -236,6 +215,7 @@ __device__ __forceinline__ void heat_oseam_body(const SweptArgs& a, const int un
         return a.xface + fo * ny + xface_col(gc, m, ny);
     };
     double f0 = 0.0, f1 = 0.0, f2 = 0.0, f3 = 0.0;
+    double p2 = 0.0, p3 = 0.0;  // lower face rows of the previous level
     for (int m = 1; m <= H; ++m) {
         // this level's x-faces, placed after the level (they are the next
         // level's rows); loaded now so the level's arithmetic covers them
@@ -246,8 +226,14 @@ __device__ __forceinline__ void heat_oseam_body(const SweptArgs& a, const int un
             f3 = *xrow(band, 0, 1, m);
         }
         // ---- level m, in place from index 2m+1 down to 2 ---------------------
-#define PSB_OSEAM_ENTRY(M) \
-    case M:                \
+        // (entering level m places the lower face rows of level m-1 at
+        // indices 2m, 2m+1; at m = 1 they are the base rows of level 0)
+#define PSB_OSEAM_ENTRY(M)                                                                 \
+    case M:                                                                                \
+        if constexpr ((M) >= 2 && 2 * (M) + 1 < BX) {                                      \
+            v[2 * (M)] = p2;                                                               \
+            v[2 * (M) + 1] = p3;                                                           \
+        }                                                                                  \
         goto orow_##M;
 #define PSB_OSEAM_ROW(K)                                                                   \
     if constexpr ((K) >= 2 && (K) < BX) {                                                  \
@@ -322,10 +308,12 @@ __device__ __forceinline__ void heat_oseam_body(const SweptArgs& a, const int un
                 if (k >= 2 * m + 2) break;
                 if (face) v[k] = src[(k - 2) * 2];
             }
-            // the prisms' face rows of level m: indices 0, 1 and 2m+2, 2m+3
+            // the prisms' face rows of level m: indices 0, 1 now, 2m+2 and
+            // 2m+3 on entering the next level
             v[0] = f0;
             v[1] = f1;
-            oseam_lower<BX>(m, f2, f3, v);
+            p2 = f2;
+            p3 = f3;
         }
     }
 }
