@@ -16,6 +16,7 @@
 
 #include "../../include/pysweep_b200.h"
 #include "heat_fast.cuh"
+#include "seam_fast.cuh"
 #include "swept.cuh"
 
 namespace {
@@ -124,8 +125,8 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
             const void* kernels[] = {
                 (const void*)heat_stream_fast<16, false>, (const void*)heat_stream_fast<16, true>,
                 (const void*)heat_stream_fast<32, false>, (const void*)heat_stream_fast<32, true>,
-                (const void*)seam_kernel<Heat, 1, false, 128>,
-                (const void*)seam_kernel<Heat, 1, true, 128>};
+                (const void*)heat_yseam_fast<16>, (const void*)heat_oseam_fast<16>,
+                (const void*)heat_yseam_fast<32>, (const void*)heat_oseam_fast<32>};
             for (const void* k : kernels) {
                 e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
                 if (e != cudaSuccess) {
@@ -168,8 +169,9 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
     const int units = nb * nseg;
     const int fgrid = (units + kFastWarps - 1) / kFastWarps;
     const size_t fsm = BX == 16 ? heat_fast_smem<16>(H) : heat_fast_smem<32>(H);
-    const size_t ssm = sizeof(double) * std::max(seam_smem_elems(false, BX, 1, 1, 1, H),
-                                                 seam_smem_elems(true, BX, 1, 1, 1, H));
+    // the register seams: one warp per block edge
+    const int sgrid = (units + kSeamWarps - 1) / kSeamWarps;
+    const size_t ssm = BX == 16 ? yseam_smem<16>(H) : yseam_smem<32>(H);
     const int64_t halves = (nsteps + H - 1) / H;
     // outputs alternate between d_out and the scratch field so that the last
     // half-cycle lands in d_out and d_in is only read
@@ -186,14 +188,14 @@ extern "C" int ps_heat_swept_noalloc(const double* d_in, double* d_out, int nx, 
         a.bout = out;
         if (BX == 16) {
             heat_stream_fast<16, false><<<fgrid, 32 * kFastWarps, fsm, st>>>(a);
-            seam_kernel<Heat, 1, false, 128><<<units, 128, ssm, st>>>(a);
+            heat_yseam_fast<16><<<sgrid, 32 * kSeamWarps, ssm, st>>>(a);
             heat_stream_fast<16, true><<<fgrid, 32 * kFastWarps, fsm, st>>>(a);
-            seam_kernel<Heat, 1, true, 128><<<units, 128, ssm, st>>>(a);
+            heat_oseam_fast<16><<<sgrid, 32 * kSeamWarps, ssm, st>>>(a);
         } else {
             heat_stream_fast<32, false><<<fgrid, 32 * kFastWarps, fsm, st>>>(a);
-            seam_kernel<Heat, 1, false, 128><<<units, 128, ssm, st>>>(a);
+            heat_yseam_fast<32><<<sgrid, 32 * kSeamWarps, ssm, st>>>(a);
             heat_stream_fast<32, true><<<fgrid, 32 * kFastWarps, fsm, st>>>(a);
-            seam_kernel<Heat, 1, true, 128><<<units, 128, ssm, st>>>(a);
+            heat_oseam_fast<32><<<sgrid, 32 * kSeamWarps, ssm, st>>>(a);
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {
