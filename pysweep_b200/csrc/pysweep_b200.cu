@@ -627,7 +627,15 @@ int run_swept(ps_solver* s, int64_t nlevels, int gts0, double* frames, int64_t f
             // leave few, long CTAs and a ragged last wave.  Measured on Euler
             // (G cell-stages/s): 1024², bs 32: 16 segments 3.00, 8: 3.31,
             // 4: 3.32; 4096², bs 16: 2: 5.65, 16: 6.26, 32: 5.93, 64: 5.39.
-            const int minw = std::max(4 * s->chunk, O2 * (s->H + 1));
+            // Step hooks keep eight chunks where that still gives every SM a
+            // CTA: their seams are the generic ones, with a slot per level
+            // (heat as a hook at 4096², Gcell-updates/s: bs 16, 32 segments
+            // 105.5, 16: 113.3; bs 32 at h 6: 128.5 and 135.6).
+            int sms = 148;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+            int minw = std::max(4 * s->chunk, O2 * (s->H + 1));
+            if (s->hook && (s->nx / s->bs) * (s->ny / (8 * s->chunk)) >= sms)
+                minw = std::max(minw, 8 * s->chunk);
             s->nseg = 1;
             for (int q = 2; s->ny / q >= minw; ++q)
                 if (s->ny % q == 0) s->nseg = q;
@@ -1094,15 +1102,22 @@ int ps_create_hook(ps_solver** out, int device, const char* source, const char* 
         s->hook->ops = ops;
         s->hook->its = its;
         s->hook_src = source;
-        // levels per half-cycle: MPSS, fewer where the hook's linear slots
-        // (one per level) would not fit in shared memory
-        s->H = s->mpss;
-        for (;;) {
-            s->chunk = (2 * ops * (s->H + 1) <= 32) ? 32 : 64;
-            const bool fits = 2 * ops * (s->H + 1) <= 64 && stream_smem(s) <= 227 * 1024 &&
-                              seam_smem(s) <= 227 * 1024;
-            if (fits || s->H == 1) break;
-            --s->H;
+        // levels per half-cycle: the most (up to MPSS) whose stream tile,
+        // one linear slot per level, leaves room for three CTAs per SM; where
+        // none does, the most that fit at all.  (The heat plugin as a hook,
+        // 4096², 600 steps, Gcell-updates/s: bs 32 at MPSS = 15, one CTA per
+        // SM, 59; at 6, three CTAs, 136; bs 16 keeps MPSS = 7.)
+        for (const size_t cap : {(size_t)227 * 1024 / 3, (size_t)227 * 1024}) {
+            s->H = s->mpss;
+            bool fits = false;
+            for (;;) {
+                s->chunk = (2 * ops * (s->H + 1) <= 32) ? 32 : 64;
+                fits = 2 * ops * (s->H + 1) <= 64 && stream_smem(s) <= cap &&
+                       seam_smem(s) <= 227 * 1024;
+                if (fits || s->H == 1) break;
+                --s->H;
+            }
+            if (fits) break;
         }
         std::vector<char> cubin;
         std::string log;
