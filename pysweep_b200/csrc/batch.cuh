@@ -18,6 +18,21 @@ namespace psb {
 // Descriptors [instance][role][parity]: role 0 for the prism stream and the
 // y-bridge, role 1 for the gap stream and the octahedron (their y-faces live in
 // a second buffer, because the gap runs beside the y-bridge).
+//
+// The register heat kernels (one warp per table entry) copy their entry's
+// descriptor into shared memory, kDescBytes per warp at the start of the
+// dynamic shared memory, and the bodies read the fields from there as the
+// single-instance kernels read their parameter-bank copy: a copy in
+// registers spilled 84-200 bytes per thread in the bs-32 streams (256 heat
+// instances of 128-2048², 1000 steps: 0.703 -> 0.615 s).  The generic
+// kernels keep a copy in registers (batch_args): for Euler the shared copy
+// measured no better.
+constexpr int kDescBytes = (int)((sizeof(SweptArgs) + 15) / 16 * 16);
+static_assert(sizeof(SweptArgs) % 8 == 0, "the descriptor copies in 8-byte words");
+
+// Threads t of [0, nt) copy descriptor `inst` into `slot`; after the callers'
+// barrier, one of them (t == 0) sets this launch's levels and first level,
+// and a second barrier publishes the copy.
 template <bool GAP>
 __device__ __forceinline__ void batch_args(const SweptArgs* __restrict__ desc, int inst,
                                            int parity, int H, long long L0, SweptArgs& a)
@@ -27,20 +42,38 @@ __device__ __forceinline__ void batch_args(const SweptArgs* __restrict__ desc, i
     a.L0 = L0;
 }
 
+template <bool GAP>
+__device__ __forceinline__ void batch_desc_copy(const SweptArgs* __restrict__ desc, int inst,
+                                                int parity, SweptArgs* slot, int t, int nt)
+{
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(
+        desc + 4 * inst + 2 * (GAP ? 1 : 0) + parity);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(slot);
+    for (int w = t; w < (int)(sizeof(SweptArgs) / 8); w += nt) dst[w] = src[w];
+}
+
 template <int BX, bool GAP>
 __global__ void __launch_bounds__(32 * kFastWarps, 3)
     heat_stream_fast_batch(const SweptArgs* __restrict__ desc, const int2* __restrict__ units,
                            int nunits, int parity, int H, long long L0)
 {
     extern __shared__ double sm[];
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = blockIdx.x * kFastWarps + warp;
     if (g >= nunits) return;  // whole warp
     const int2 u = units[g];
-    SweptArgs a;
-    batch_args<GAP>(desc, u.x, parity, H, L0, a);
+    SweptArgs* slot = reinterpret_cast<SweptArgs*>(reinterpret_cast<char*>(sm) + warp * kDescBytes);
+    batch_desc_copy<GAP>(desc, u.x, parity, slot, lane, 32);
+    __syncwarp();
+    if (lane == 0) {
+        slot->H = H;
+        slot->L0 = L0;
+    }
+    __syncwarp();
+    const SweptArgs& a = *slot;
+    double* base = sm + kFastWarps * kDescBytes / 8;
     heat_fast_body<BX, GAP>(a, seg_geom(a, u.y), u.y,
-                            sm + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
+                            base + (size_t)warp * heat_fast_warp_doubles<BX>(a.Hmax));
 }
 
 // The register-resident heat seams (seam_fast.cuh) over the unit table: one
@@ -51,13 +84,20 @@ __global__ void __launch_bounds__(32 * kSeamWarps)
                          int nunits, int parity, int H, long long L0)
 {
     extern __shared__ double sm[];
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = blockIdx.x * kSeamWarps + warp;
     if (g >= nunits) return;  // whole warp
     const int2 u = units[g];
-    SweptArgs a;
-    batch_args<GAP>(desc, u.x, parity, H, L0, a);
-    double* ys = sm + (size_t)warp * yseam_warp_doubles<BX>(a.Hmax);
+    SweptArgs* slot = reinterpret_cast<SweptArgs*>(reinterpret_cast<char*>(sm) + warp * kDescBytes);
+    batch_desc_copy<GAP>(desc, u.x, parity, slot, lane, 32);
+    __syncwarp();
+    if (lane == 0) {
+        slot->H = H;
+        slot->L0 = L0;
+    }
+    __syncwarp();
+    const SweptArgs& a = *slot;
+    double* ys = sm + kSeamWarps * kDescBytes / 8 + (size_t)warp * yseam_warp_doubles<BX>(a.Hmax);
     if constexpr (GAP)
         heat_oseam_body<BX>(a, u.y, ys);
     else

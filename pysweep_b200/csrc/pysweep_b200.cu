@@ -1481,7 +1481,7 @@ struct ps_batch {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<BatchInst> inst;
-    SweptArgs* d_desc = nullptr;  // [count][2 roles][2 parities] (batch_args)
+    SweptArgs* d_desc = nullptr;  // [count][2 roles][2 parities] (batch.cuh)
     int2* d_units = nullptr;      // (instance, unit) of every band segment
     int nunits = 0;
     int cur = 0;                  // base holding the current levels (all instances)
@@ -1655,7 +1655,8 @@ void batch_half(ps_batch* b, int par, int H, long long L0, size_t ssm, size_t gs
     if (b->fast) {
         // the register-resident seams, one warp per unit
         const dim3 sgrid((nu + kSeamWarps - 1) / kSeamWarps);
-        const size_t ysm = b->bs == 16 ? yseam_smem<16>(b->H) : yseam_smem<32>(b->H);
+        const size_t ysm =
+            (b->bs == 16 ? yseam_smem<16>(b->H) : yseam_smem<32>(b->H)) + kSeamWarps * kDescBytes;
         if (b->bs == 16) {
             heat_seam_fast_batch<16, false><<<sgrid, 32 * kSeamWarps, ysm, st>>>(b->d_desc, b->d_units, nu, par, H, L0);
             join();
@@ -1713,7 +1714,10 @@ bool batch_pick(int eq, int ops, int its, int chunk, HalfFn* half, PrepFn* prep)
 // Enqueue a whole run of nlevels levels, starting from parity b->cur.
 int batch_enqueue(ps_batch* b, int64_t nlevels, HalfFn half, int64_t* nlaunch)
 {
-    const size_t ssm = batch_seam_smem(b), gsm = batch_stream_smem(b);
+    // (the register heat streams' descriptor copies come first in their
+    // shared memory)
+    const size_t ssm = batch_seam_smem(b),
+                 gsm = batch_stream_smem(b) + (b->fast ? kFastWarps * kDescBytes : 0);
     const dim3 fgrid((b->nunits + kFastWarps - 1) / kFastWarps);
     const size_t fe = (size_t)b->nv;
     int par = b->cur;
