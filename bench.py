@@ -453,7 +453,7 @@ def hook_line(args, n=4096, steps=600):
     g = heat_globals(n, steps)
     d_ic = torch.from_numpy(ic).cuda()
     out, res = {}, {}
-    for label, eq, bs in (("hook", hook, 16), ("builtin", "heat", 32)):
+    for label, eq, bs in (("hook", hook, 32), ("builtin", "heat", 32)):
         e = Engine(eq, n, n, blocksize=bs)
         for k, v in plugin_constants("heat", g).items():
             e.set_global(k, v)
@@ -474,7 +474,7 @@ def hook_line(args, n=4096, steps=600):
         e.close()
     return {"metric": "step hook Gcell-updates/s FP64 (heat in the plugin format, NVRTC)",
             "unit": "Gcell-updates/s", "n": n, "time_steps": steps,
-            "hook_blocksize": 16, "builtin_blocksize": 32,
+            "hook_blocksize": 32, "builtin_blocksize": 32,
             "hook_swept": res[("hook", "swept")], "hook_standard": res[("hook", "standard")],
             "builtin_swept": res[("builtin", "swept")],
             "builtin_standard": res[("builtin", "standard")],
