@@ -453,7 +453,9 @@ __device__ __forceinline__ void gap_entry(const double (&a1)[BX], const double* 
 // segment's y-faces; `carry` is the warp's own shared memory
 // (heat_fast_warp_doubles: two packed carry buffers, then the ring).
 // T: storage type of the fields and faces (double or float).
-template <int BX, bool GAP, class T = double, int VAR = 0>
+// MINROWS: rows every prism level is known to keep (BX - 2h for h levels per
+// half-cycle); the row loop tests for the level's end only past them.
+template <int BX, bool GAP, class T = double, int VAR = 0, int MINROWS = 2>
 __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom sg,
                                                const int unit, double* carry)
 {
@@ -586,7 +588,7 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
                 }
 #pragma unroll
                 for (int i = 0; i < BX - 2; ++i) {
-                    if (i >= count) break;
+                    if (i >= MINROWS && i >= count) break;
                     const double2 cd = *reinterpret_cast<const double2*>(cr0 + (i + 2) * 2);
                     const double L1d = from_left(a1[i + 2], cd.y, lane);
                     const double L0c = from_left(a0[i + 1], cc.x, lane);
@@ -743,14 +745,14 @@ __device__ __forceinline__ void heat_fast_body(const SweptArgs& a, const SegGeom
 // VAR 0: heat (one courant number); VAR 1: a courant number per cell
 // (HeatVar), storing each old level's Laplacian when p.f[1] is set; VAR 2: the
 // adjoint in mu = C .* lambda (HeatVarAdjMu).
-template <int BX, bool GAP, class T = double, int VAR = 0>
+template <int BX, bool GAP, class T = double, int VAR = 0, int MINROWS = 2>
 __global__ void __launch_bounds__(32 * kFastWarps, kFastCtasPerSm<BX, VAR>) heat_stream_fast(SweptArgs a)
 {
     extern __shared__ double sm[];
     const int warp = threadIdx.x >> 5;
     const int unit = blockIdx.x * kFastWarps + warp;
     if (unit >= a.nb * a.nseg) return;  // whole warp leaves together
-    heat_fast_body<BX, GAP, T, VAR>(a, seg_geom(a, unit), unit,
+    heat_fast_body<BX, GAP, T, VAR, MINROWS>(a, seg_geom(a, unit), unit,
                                     sm + (size_t)warp * heat_fast_warp_doubles_v<BX, VAR>(a.Hmax));
 }
 
