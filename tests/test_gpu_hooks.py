@@ -76,6 +76,34 @@ def test_hook_tiling_changes_no_bit():
         assert np.array_equal(got, ref), cfg
 
 
+def test_hook_default_tiling_keeps_three_ctas_per_sm():
+    """A one-variable hook at blocksize 32 defaults to 6 levels per
+    half-cycle (the most whose stream tile, one linear slot per level, leaves
+    room for three CTAs per SM), not MPSS = 15; both give the same bits."""
+    import torch
+    from pysweep_b200 import Engine, plugin_constants
+    path = os.path.join(HOOKS, "heat_numpy_order.cu")
+    n, nl = 256, 40
+    ic = np.random.default_rng(5).standard_normal((1, n, n))
+    dx = 1.0 / n
+    g = [0.0, nl * 0.2 * dx * dx, 0.2 * dx * dx, dx, dx, 1.0, True]
+    out = {}
+    for h in (0, 15):
+        e = Engine(path, n, n, blocksize=32)
+        for k, v in plugin_constants("heat", g).items():
+            e.set_global(k, v)
+        if h:
+            e.configure(h=h)
+        else:
+            assert e.tiling()["h"] == 6 and e.tiling()["mpss"] == 15
+        e.set_state(ic)
+        e.run(nl, mode="swept")
+        out[h] = e.get_state()
+        e.close()
+    torch.cuda.synchronize()
+    assert np.array_equal(out[0], out[15])
+
+
 def _wave_numpy(u0, v0, a, dt, nlevels):
     """tests/hooks/wave4.cu restated on whole arrays, in the hook's order."""
     def d1(f, ax):
