@@ -30,9 +30,8 @@ namespace psb {
 constexpr int kDescBytes = (int)((sizeof(SweptArgs) + 15) / 16 * 16);
 static_assert(sizeof(SweptArgs) % 8 == 0, "the descriptor copies in 8-byte words");
 
-// Threads t of [0, nt) copy descriptor `inst` into `slot`; after the callers'
-// barrier, one of them (t == 0) sets this launch's levels and first level,
-// and a second barrier publishes the copy.
+// The generic kernels' register copy, with this launch's levels and first
+// level.
 template <bool GAP>
 __device__ __forceinline__ void batch_args(const SweptArgs* __restrict__ desc, int inst,
                                            int parity, int H, long long L0, SweptArgs& a)
@@ -42,6 +41,9 @@ __device__ __forceinline__ void batch_args(const SweptArgs* __restrict__ desc, i
     a.L0 = L0;
 }
 
+// Threads t of [0, nt) copy descriptor `inst` into `slot`; after the callers'
+// barrier, one of them (t == 0) sets this launch's levels and first level,
+// and a second barrier publishes the copy.
 template <bool GAP>
 __device__ __forceinline__ void batch_desc_copy(const SweptArgs* __restrict__ desc, int inst,
                                                 int parity, SweptArgs* slot, int t, int nt)
